@@ -1,0 +1,603 @@
+// C ABI of the library (include/bnm_b200.h): configuration, plans, the batch
+// entry point and its one-shot run_simulations mirror.
+//
+// A plan allocates every device buffer once for max_sims particles and then
+// runs a generation as a fixed sequence of launches on its own stream:
+//   analytic FIC (optional) -> integrate -> FC + window FC -> FCD + KS histogram -> GOF
+// (the reference runs bnm, bold_stats, window_bold_stats, fc, window_fc_stats,
+// fcd, float2double with a device-wide sync after each, then a host GOF loop,
+// bnm.cu:623-769).  Errors come back as status codes, never exit().
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "../../include/bnm_b200.h"
+#include "kernels.h"
+
+using namespace bnm;
+
+static thread_local std::string g_err;
+
+static int fail(int code, const char* fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+int bnm_fail_cuda(cudaError_t e, const char* expr, const char* file, int line) {
+    return fail(e == cudaErrorMemoryAllocation ? BNM_ENOMEM : BNM_ECUDA, "%s failed: %s (%s:%d)", expr,
+                cudaGetErrorString(e), file, line);
+}
+
+extern "C" const char* bnm_last_error(void) { return g_err.c_str(); }
+
+extern "C" int bnm_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) return 0;
+    return n;
+}
+
+extern "C" void bnm_config_default(bnm_config* c) {
+    std::memset(c, 0, sizeof *c);
+    c->nodes = 100;
+    c->max_sims = 1;
+    c->time_steps = 60000;
+    c->bold_tr = 1000;
+    c->window_step = 2;
+    c->window_size = 10;
+    c->bold_remove_s = 30;
+    c->exc_interhem = 1;
+    c->do_fic = 1;
+    c->numerical_fic = 1;
+    c->max_fic_trials = 10;
+    c->i_sampling_start = 1000;
+    c->i_sampling_end = 10000;
+    c->init_delta = (double)(float)0.02;
+    c->use_fc_diff = 1;
+    c->fic_reject_failed = 0;
+    c->fic_penalty_scale = 2.0;
+    c->max_cost = 2.0;
+    c->calculate_fic_penalty = 1;
+    c->no_fcd = 0;
+    c->precision = BNM_PREC_F32;
+    c->noise_mode = BNM_NOISE_PHILOX;
+    c->noise_seed = 410;
+    c->device = 0;
+}
+
+// helpers.cpp:4-19: ints through atoi; doubles through atof, returned as float.
+static int env_int(const char* k, int d) {
+    const char* v = std::getenv(k);
+    return v ? std::atoi(v) : d;
+}
+static double env_dbl(const char* k, double d) {
+    const char* v = std::getenv(k);
+    return v ? (double)(float)std::atof(v) : (double)(float)d;
+}
+
+extern "C" void bnm_config_from_env(bnm_config* c) {
+    c->bold_remove_s = env_int("BNM_BOLD_REMOVE", c->bold_remove_s);
+    c->max_cost = (double)env_int("BNM_MAX_COST", (int)c->max_cost);
+    c->i_sampling_start = env_int("BNM_I_SAMPLING_START", c->i_sampling_start);
+    c->i_sampling_end = env_int("BNM_I_SAMPLING_END", c->i_sampling_end);
+    c->numerical_fic = env_int("BNM_NUMERICAL_FIC", c->numerical_fic) != 0;
+    c->max_fic_trials = env_int("BNM_MAX_FIC_TRIALS_CMAES", c->max_fic_trials);
+    c->init_delta = env_dbl("BNM_INIT_DELTA", 0.02);
+    c->use_fc_diff = env_int("BNM_USE_FC_DIFF", c->use_fc_diff) != 0;
+    c->exc_interhem = env_int("BNM_EXC_INTERHEM", c->exc_interhem) != 0;
+    c->fic_penalty_scale = env_dbl("BNM_CMAES_FIC_PENALTY_SCALE", 2.0);
+    c->fic_reject_failed = env_int("BNM_CMAES_FIC_REJECT_FAILED", c->fic_reject_failed) != 0;
+}
+
+// Sizes of run_CMAES.cpp:476-594.
+extern "C" int bnm_config_sizes(const bnm_config* c, bnm_sizes* s) {
+    if (c->nodes < 2 || c->nodes > 1024) return fail(BNM_EINVAL, "nodes must be in [2, 1024] (got %d)", c->nodes);
+    if (c->bold_tr <= 0 || c->time_steps < 0) return fail(BNM_EINVAL, "time_steps >= 0 and BOLD_TR > 0 required");
+    if (c->window_step <= 0 || c->window_size < 0) return fail(BNM_EINVAL, "window_step > 0 and window_size >= 0 required");
+    if (c->exc_interhem && (c->nodes % 2)) return fail(BNM_EINVAL, "exc_interhem needs an even node count");
+    std::memset(s, 0, sizeof *s);
+    s->frames = c->time_steps / c->bold_tr + 1;
+    // the reference sizes its buffers with a floating-point quotient
+    // (run_CMAES.cpp:476-477); frames are written at ts % TR == 0, so the two
+    // must agree or the reference itself would under/overrun.
+    const double tr_s = (double)c->bold_tr / 1000;
+    const int ref_frames = (int)(c->time_steps / (tr_s / 0.001)) + 1;
+    if (ref_frames != s->frames)
+        return fail(BNM_EINVAL, "time_steps/BOLD_TR gives %d frames but the reference sizes %d", s->frames, ref_frames);
+    s->n_vols_remove = c->bold_remove_s * 1000 / c->bold_tr;
+    s->corr_len = s->frames - s->n_vols_remove;
+    if (s->corr_len < 2) return fail(BNM_EINVAL, "fewer than 2 BOLD frames left after removing %d", s->n_vols_remove);
+    const int N = c->nodes;
+    s->n_pairs = N * (N - 1) / 2 - (c->exc_interhem ? (N / 2) * (N / 2) : 0);
+    const int h = c->window_size / 2;
+    s->window_len = 2 * h + 1;
+    const int first = h, last = s->corr_len - 1 - h;
+    s->n_windows = last >= first ? (last - first) / c->window_step + 1 : 0;
+    s->n_fcd = s->n_windows * (s->n_windows - 1) / 2;
+    if (!c->no_fcd && s->n_windows < 2) return fail(BNM_EINVAL, "need at least 2 FCD windows (got %d)", s->n_windows);
+    s->noise_len = (int64_t)N * (c->time_steps + 1) * 10 * 2;
+    return BNM_OK;
+}
+
+struct bnm_plan {
+    bnm_config cfg;
+    bnm_sizes sz;
+    int num_sms = 0, kmax = 0, sc_ld = 0, m = 0;
+    cudaStream_t st = nullptr;
+    cudaEvent_t ev[6] = {};
+    double emp_fc_mean = 0;
+    float* d_sc32 = nullptr;
+    double *d_sc64 = nullptr, *d_sc_fic = nullptr;
+    float* d_noise = nullptr;
+    int *d_pi = nullptr, *d_pj = nullptr;
+    double *d_emp_fc = nullptr, *d_emp_sorted = nullptr;
+    unsigned char* d_valid = nullptr;
+    double *d_G = nullptr, *d_wEE = nullptr, *d_wEI = nullptr, *d_wIE = nullptr, *d_wIE_out = nullptr;
+    int* d_unstable = nullptr;
+    float* d_bold = nullptr;
+    double* d_bold64 = nullptr;
+    int *d_trials = nullptr, *d_failed = nullptr, *d_nan = nullptr, *d_counter = nullptr, *d_status = nullptr;
+    double* d_ext = nullptr;
+    float *d_fc = nullptr, *d_wfc = nullptr, *d_fcd = nullptr;
+    double* d_wsum = nullptr;
+    unsigned int *d_hist = nullptr, *d_eq = nullptr;
+    double *d_cost = nullptr, *d_pen = nullptr, *d_fcc = nullptr, *d_fcdiff = nullptr, *d_ks = nullptr;
+    double timings[6] = {0, 0, 0, 0, 0, 0};
+    std::vector<void*> allocs;
+};
+
+template <typename T>
+static cudaError_t dalloc(bnm_plan* p, T** ptr, size_t count) {
+    cudaError_t e = cudaMalloc((void**)ptr, std::max<size_t>(count, 1) * sizeof(T));
+    if (e == cudaSuccess) p->allocs.push_back(*ptr);
+    return e;
+}
+
+extern "C" void bnm_plan_destroy(bnm_plan* p) {
+    if (!p) return;
+    cudaSetDevice(p->cfg.device);
+    if (p->st) cudaStreamSynchronize(p->st);
+    for (void* a : p->allocs) cudaFree(a);
+    for (auto& e : p->ev)
+        if (e) cudaEventDestroy(e);
+    if (p->st) cudaStreamDestroy(p->st);
+    delete p;
+}
+
+static int plan_create(const bnm_config* cfg, const double* sc, const double* emp_fc, int n_emp_fc,
+                       const double* emp_fcd, int n_emp_fcd, const float* host_noise, int64_t n_host_noise,
+                       bnm_plan* p) {
+    p->cfg = *cfg;
+    int rc = bnm_config_sizes(cfg, &p->sz);
+    if (rc) return rc;
+    const bnm_sizes& s = p->sz;
+    const int N = cfg->nodes;
+    if (cfg->max_sims < 1) return fail(BNM_EINVAL, "max_sims must be >= 1");
+    if (!sc) return fail(BNM_EINVAL, "SC is required");
+    if (!emp_fc || n_emp_fc != s.n_pairs)
+        return fail(BNM_EINVAL, "empirical FC has %d values; %d nodes with exc_interhem=%d need %d", n_emp_fc, N,
+                    cfg->exc_interhem, s.n_pairs);
+    if (!cfg->no_fcd && (!emp_fcd || n_emp_fcd < 1)) return fail(BNM_EINVAL, "empirical FCD is required");
+    if (cfg->noise_mode == BNM_NOISE_HOST && (!host_noise || n_host_noise < s.noise_len))
+        return fail(BNM_EINVAL, "host noise needs %lld values (got %lld)", (long long)s.noise_len,
+                    (long long)n_host_noise);
+    if (cfg->precision < 0 || cfg->precision > 2) return fail(BNM_EINVAL, "unknown precision %d", cfg->precision);
+    for (int i = 0; i < N * N; i++)
+        if (!std::isfinite(sc[i])) return fail(BNM_EINVAL, "SC has a non-finite entry at %d", i);
+
+    BNM_CUDA_TRY(cudaSetDevice(cfg->device));
+    BNM_CUDA_TRY(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, cfg->device));
+    BNM_CUDA_TRY(cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking));
+    for (auto& e : p->ev) BNM_CUDA_TRY(cudaEventCreate(&e));
+
+    // SC: FP32 rows padded for the register kernel, FP64 for the exact kernel,
+    // and the FIC copy rounded like the chosen precision's u_real.
+    p->kmax = (cfg->precision == BNM_PREC_F32) ? bnm_fast_kmax(N) : 0;
+    p->sc_ld = p->kmax ? p->kmax : N;
+    std::vector<float> sc32((size_t)N * p->sc_ld, 0.f);
+    std::vector<double> scfic((size_t)N * N);
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < N; j++) {
+            sc32[(size_t)i * p->sc_ld + j] = (float)sc[(size_t)i * N + j];
+            scfic[(size_t)i * N + j] =
+                cfg->precision == BNM_PREC_F32_REF ? (double)(float)sc[(size_t)i * N + j] : sc[(size_t)i * N + j];
+        }
+    BNM_CUDA_TRY(dalloc(p, &p->d_sc32, sc32.size()));
+    BNM_CUDA_TRY(dalloc(p, &p->d_sc64, (size_t)N * N));
+    BNM_CUDA_TRY(dalloc(p, &p->d_sc_fic, (size_t)N * N));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_sc32, sc32.data(), sc32.size() * 4, cudaMemcpyHostToDevice));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_sc64, sc, (size_t)N * N * 8, cudaMemcpyHostToDevice));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_sc_fic, scfic.data(), scfic.size() * 8, cudaMemcpyHostToDevice));
+
+    // noise table
+    BNM_CUDA_TRY(dalloc(p, &p->d_noise, (size_t)s.noise_len));
+    if (cfg->noise_mode == BNM_NOISE_HOST) {
+        BNM_CUDA_TRY(cudaMemcpy(p->d_noise, host_noise, (size_t)s.noise_len * 4, cudaMemcpyHostToDevice));
+    } else {
+        BNM_CUDA_TRY(bnm_launch_philox(p->d_noise, (uint64_t)s.noise_len, cfg->noise_seed, p->num_sms, p->st));
+    }
+
+    // pair table (run_CMAES.cpp:505-524)
+    std::vector<int> pi, pj;
+    const int rh = N / 2;
+    for (int i = 0; i < N; i++)
+        for (int j = 0; j < i; j++) {
+            if (cfg->exc_interhem && ((i < rh) ^ (j < rh))) continue;
+            pi.push_back(i);
+            pj.push_back(j);
+        }
+    BNM_CUDA_TRY(dalloc(p, &p->d_pi, pi.size()));
+    BNM_CUDA_TRY(dalloc(p, &p->d_pj, pj.size()));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_pi, pi.data(), pi.size() * 4, cudaMemcpyHostToDevice));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_pj, pj.data(), pj.size() * 4, cudaMemcpyHostToDevice));
+
+    // targets: empirical FC and its mean; empirical FCD sorted, with jump flags
+    double mfc = 0;
+    for (int i = 0; i < n_emp_fc; i++) mfc += emp_fc[i];
+    p->emp_fc_mean = mfc / n_emp_fc;
+    BNM_CUDA_TRY(dalloc(p, &p->d_emp_fc, n_emp_fc));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_emp_fc, emp_fc, (size_t)n_emp_fc * 8, cudaMemcpyHostToDevice));
+    p->m = cfg->no_fcd ? 1 : n_emp_fcd;
+    std::vector<double> es(p->m, 0.0);
+    if (!cfg->no_fcd) {
+        es.assign(emp_fcd, emp_fcd + n_emp_fcd);
+        std::sort(es.begin(), es.end());
+    }
+    std::vector<unsigned char> valid(p->m + 1, 0);
+    valid[0] = 1;  // sims below every empirical value
+    for (int c = 1; c <= p->m; c++) valid[c] = (c == p->m) || (es[c - 1] < es[c]);
+    BNM_CUDA_TRY(dalloc(p, &p->d_emp_sorted, es.size()));
+    BNM_CUDA_TRY(dalloc(p, &p->d_valid, valid.size()));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_emp_sorted, es.data(), es.size() * 8, cudaMemcpyHostToDevice));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_valid, valid.data(), valid.size(), cudaMemcpyHostToDevice));
+
+    // per-particle work space
+    const size_t n = cfg->max_sims;
+    BNM_CUDA_TRY(dalloc(p, &p->d_G, n));
+    BNM_CUDA_TRY(dalloc(p, &p->d_wEE, n * N));
+    BNM_CUDA_TRY(dalloc(p, &p->d_wEI, n * N));
+    BNM_CUDA_TRY(dalloc(p, &p->d_wIE, n * N));
+    BNM_CUDA_TRY(dalloc(p, &p->d_wIE_out, n * N));
+    BNM_CUDA_TRY(dalloc(p, &p->d_unstable, n));
+    if (cfg->precision == BNM_PREC_F64)
+        BNM_CUDA_TRY(dalloc(p, &p->d_bold64, n * s.frames * N));
+    else
+        BNM_CUDA_TRY(dalloc(p, &p->d_bold, n * s.frames * N));
+    BNM_CUDA_TRY(dalloc(p, &p->d_trials, n));
+    BNM_CUDA_TRY(dalloc(p, &p->d_failed, n));
+    BNM_CUDA_TRY(dalloc(p, &p->d_nan, n));
+    BNM_CUDA_TRY(dalloc(p, &p->d_counter, 4));
+    BNM_CUDA_TRY(dalloc(p, &p->d_status, 4));
+    BNM_CUDA_TRY(dalloc(p, &p->d_ext, n * 6 * N));
+    BNM_CUDA_TRY(dalloc(p, &p->d_fc, n * s.n_pairs));
+    BNM_CUDA_TRY(dalloc(p, &p->d_wfc, n * (size_t)std::max(s.n_windows, 1) * s.n_pairs));
+    BNM_CUDA_TRY(dalloc(p, &p->d_wsum, n * (size_t)std::max(s.n_windows, 1) * 2));
+    BNM_CUDA_TRY(dalloc(p, &p->d_fcd, n * (size_t)std::max(s.n_fcd, 1)));
+    BNM_CUDA_TRY(dalloc(p, &p->d_hist, n * (size_t)(p->m + 1)));
+    BNM_CUDA_TRY(dalloc(p, &p->d_eq, n * (size_t)(p->m + 1)));
+    BNM_CUDA_TRY(dalloc(p, &p->d_cost, n));
+    BNM_CUDA_TRY(dalloc(p, &p->d_pen, n));
+    BNM_CUDA_TRY(dalloc(p, &p->d_fcc, n));
+    BNM_CUDA_TRY(dalloc(p, &p->d_fcdiff, n));
+    BNM_CUDA_TRY(dalloc(p, &p->d_ks, n));
+    BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
+    return BNM_OK;
+}
+
+extern "C" int bnm_plan_create(const bnm_config* cfg, const double* sc, const double* emp_fc, int32_t n_emp_fc,
+                               const double* emp_fcd, int32_t n_emp_fcd, const float* host_noise,
+                               int64_t n_host_noise, bnm_plan** out) {
+    if (!cfg || !out) return fail(BNM_EINVAL, "null argument");
+    *out = nullptr;
+    bnm_plan* p = new bnm_plan();
+    int rc = plan_create(cfg, sc, emp_fc, n_emp_fc, emp_fcd, n_emp_fcd, host_noise, n_host_noise, p);
+    if (rc) {
+        bnm_plan_destroy(p);
+        return rc;
+    }
+    *out = p;
+    return BNM_OK;
+}
+
+static std::vector<double> rounded(const double* v, size_t n, bool to_float) {
+    std::vector<double> r(v, v + n);
+    if (to_float)
+        for (auto& x : r) x = (double)(float)x;
+    return r;
+}
+
+template <typename T>
+static int d2h(T* host, const T* dev, size_t n, cudaStream_t st) {
+    if (!host) return BNM_OK;
+    BNM_CUDA_TRY(cudaMemcpyAsync(host, dev, n * sizeof(T), cudaMemcpyDeviceToHost, st));
+    return BNM_OK;
+}
+
+static int f2d(double* host, const float* dev, size_t n, cudaStream_t st) {
+    if (!host) return BNM_OK;
+    std::vector<float> tmp(n);
+    BNM_CUDA_TRY(cudaMemcpyAsync(tmp.data(), dev, n * 4, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaStreamSynchronize(st));
+    for (size_t i = 0; i < n; i++) host[i] = tmp[i];
+    return BNM_OK;
+}
+
+static int launch_fic(bnm_plan* p, int n) {
+    FicArgs fa;
+    fa.n_sims = n;
+    fa.N = p->cfg.nodes;
+    fa.sc = p->d_sc_fic;
+    fa.G = p->d_G;
+    fa.wEE = p->d_wEE;
+    fa.wEI = p->d_wEI;
+    fa.wIE = p->d_wIE;
+    fa.unstable = p->d_unstable;
+    fa.fp32_consts = p->cfg.precision == BNM_PREC_F32_REF;
+    BNM_CUDA_TRY(bnm_launch_analytic_fic(fa, p->st));
+    return BNM_OK;
+}
+
+static int upload_params(bnm_plan* p, int n, const double* G, const double* w_ee, const double* w_ei) {
+    const int N = p->cfg.nodes;
+    const bool rf = p->cfg.precision == BNM_PREC_F32_REF;
+    for (int i = 0; i < n; i++)
+        if (!std::isfinite(G[i])) return fail(BNM_EINVAL, "G[%d] is not finite", i);
+    for (size_t i = 0; i < (size_t)n * N; i++)
+        if (!std::isfinite(w_ee[i]) || !std::isfinite(w_ei[i])) return fail(BNM_EINVAL, "wEE/wEI not finite at %zu", i);
+    auto g = rounded(G, n, rf), we = rounded(w_ee, (size_t)n * N, rf), wi = rounded(w_ei, (size_t)n * N, rf);
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->d_G, g.data(), n * 8, cudaMemcpyHostToDevice, p->st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->d_wEE, we.data(), (size_t)n * N * 8, cudaMemcpyHostToDevice, p->st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->d_wEI, wi.data(), (size_t)n * N * 8, cudaMemcpyHostToDevice, p->st));
+    BNM_CUDA_TRY(cudaStreamSynchronize(p->st));  // host vectors go out of scope
+    return BNM_OK;
+}
+
+extern "C" int bnm_analytic_fic(bnm_plan* p, int32_t n, const double* G, const double* w_ee, const double* w_ei,
+                                double* w_ie_out, int32_t* unstable_out) {
+    if (!p || n < 1 || n > p->cfg.max_sims) return fail(BNM_EINVAL, "n must be in [1, max_sims]");
+    BNM_CUDA_TRY(cudaSetDevice(p->cfg.device));
+    int rc = upload_params(p, n, G, w_ee, w_ei);
+    if (rc) return rc;
+    if ((rc = launch_fic(p, n))) return rc;
+    if ((rc = d2h(w_ie_out, p->d_wIE, (size_t)n * p->cfg.nodes, p->st))) return rc;
+    if ((rc = d2h(unstable_out, p->d_unstable, n, p->st))) return rc;
+    BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
+    return BNM_OK;
+}
+
+extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_ee, const double* w_ei,
+                       const double* w_ie, bnm_batch_out* out) {
+    if (!p || !out || !G || !w_ee || !w_ei) return fail(BNM_EINVAL, "null argument");
+    if (n < 1 || n > p->cfg.max_sims) return fail(BNM_EINVAL, "n=%d outside [1, max_sims=%d]", n, p->cfg.max_sims);
+    const bnm_config& c = p->cfg;
+    const bnm_sizes& s = p->sz;
+    const int N = c.nodes;
+    if (!c.do_fic && !w_ie) return fail(BNM_EINVAL, "w_ie is required when do_fic == 0");
+    BNM_CUDA_TRY(cudaSetDevice(c.device));
+    int rc = upload_params(p, n, G, w_ee, w_ei);
+    if (rc) return rc;
+    cudaStream_t st = p->st;
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[0], st));
+    const bool device_fic = c.do_fic && !w_ie;
+    if (device_fic) {
+        if ((rc = launch_fic(p, n))) return rc;
+    } else {
+        auto wi = rounded(w_ie, (size_t)n * N, c.precision == BNM_PREC_F32_REF);
+        for (double v : wi)
+            if (!std::isfinite(v)) return fail(BNM_EINVAL, "wIE not finite");
+        BNM_CUDA_TRY(cudaMemcpyAsync(p->d_wIE, wi.data(), wi.size() * 8, cudaMemcpyHostToDevice, st));
+        BNM_CUDA_TRY(cudaMemsetAsync(p->d_unstable, 0, n * 4, st));
+        BNM_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[1], st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, 16, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_nan, 0, n * 4, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_wsum, 0, (size_t)n * std::max(s.n_windows, 1) * 2 * 8, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_hist, 0, (size_t)n * (p->m + 1) * 4, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_eq, 0, (size_t)n * (p->m + 1) * 4, st));
+
+    SimArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.N = N;
+    a.n_sims = n;
+    a.T = c.time_steps;
+    a.TR = c.bold_tr;
+    a.frames = s.frames;
+    a.n_vols_remove = s.n_vols_remove;
+    a.adjust_fic = c.do_fic && c.numerical_fic;
+    a.max_trials = c.max_fic_trials;
+    a.samp_start = c.i_sampling_start;
+    a.samp_end = c.i_sampling_end;
+    a.init_delta = c.init_delta;
+    a.G = p->d_G;
+    a.wEE = p->d_wEE;
+    a.wEI = p->d_wEI;
+    a.wIE = p->d_wIE;
+    a.noise = p->d_noise;
+    a.sc_f32 = p->d_sc32;
+    a.sc_f64 = p->d_sc64;
+    a.sc_ld = p->sc_ld;
+    a.bold = p->d_bold;
+    a.bold_f64 = p->d_bold64;
+    a.wIE_out = p->d_wIE_out;
+    a.trials = p->d_trials;
+    a.failed = p->d_failed;
+    a.ext = p->d_ext;
+    a.work_counter = p->d_counter;
+    a.status = p->d_status;
+    if (c.precision == BNM_PREC_F32)
+        BNM_CUDA_TRY(bnm_launch_integrate_f32(a, p->num_sms, st));
+    else
+        BNM_CUDA_TRY(bnm_launch_integrate_exact(a, c.precision == BNM_PREC_F64, p->num_sms, st));
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[2], st));
+
+    FcArgs fa;
+    fa.N = N;
+    fa.n_sims = n;
+    fa.frames = s.frames;
+    fa.n_vols_remove = s.n_vols_remove;
+    fa.corr_len = s.corr_len;
+    fa.P = s.n_pairs;
+    fa.pair_i = p->d_pi;
+    fa.pair_j = p->d_pj;
+    fa.W = c.no_fcd ? 0 : s.n_windows;
+    fa.win_len = s.window_len;
+    fa.win_step = c.window_step;
+    fa.bold = p->d_bold;
+    fa.bold_f64 = p->d_bold64;
+    fa.fc = p->d_fc;
+    fa.wfc = p->d_wfc;
+    fa.wsum = p->d_wsum;
+    fa.nan_flag = p->d_nan;
+    BNM_CUDA_TRY(bnm_launch_fc_window(fa, st));
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[3], st));
+
+    if (!c.no_fcd) {
+        FcdArgs da;
+        da.n_sims = n;
+        da.W = s.n_windows;
+        da.P = s.n_pairs;
+        da.wfc = p->d_wfc;
+        da.wsum = p->d_wsum;
+        da.fcd = p->d_fcd;
+        da.n_fcd = s.n_fcd;
+        da.emp_sorted = p->d_emp_sorted;
+        da.m = p->m;
+        da.hist = p->d_hist;
+        da.eq = p->d_eq;
+        da.nan_flag = p->d_nan;
+        BNM_CUDA_TRY(bnm_launch_fcd(da, st));
+    }
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[4], st));
+
+    GofArgs ga;
+    ga.n_sims = n;
+    ga.N = N;
+    ga.P = s.n_pairs;
+    ga.n_fcd = s.n_fcd;
+    ga.m = p->m;
+    ga.fc = p->d_fc;
+    ga.emp_fc = p->d_emp_fc;
+    ga.emp_fc_mean = p->emp_fc_mean;
+    ga.hist = p->d_hist;
+    ga.eq = p->d_eq;
+    ga.valid = p->d_valid;
+    ga.ext = p->d_ext;
+    ga.failed = p->d_failed;
+    ga.nan_flag = p->d_nan;
+    ga.use_fc_diff = c.use_fc_diff;
+    ga.calc_fic_penalty = c.calculate_fic_penalty;
+    ga.fic_reject_failed = c.fic_reject_failed;
+    ga.no_fcd = c.no_fcd;
+    ga.max_cost = c.max_cost;
+    ga.fic_penalty_scale = c.fic_penalty_scale;
+    ga.cost = p->d_cost;
+    ga.fic_penalty = p->d_pen;
+    ga.fc_corr = p->d_fcc;
+    ga.fc_diff = p->d_fcdiff;
+    ga.fcd_ks = p->d_ks;
+    BNM_CUDA_TRY(bnm_launch_gof(ga, st));
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[5], st));
+
+    int status = 0;
+    BNM_CUDA_TRY(cudaMemcpyAsync(&status, p->d_status, 4, cudaMemcpyDeviceToHost, st));
+    if ((rc = d2h(out->cost, p->d_cost, n, st))) return rc;
+    if ((rc = d2h(out->fic_penalty, p->d_pen, n, st))) return rc;
+    if ((rc = d2h(out->fc_corr, p->d_fcc, n, st))) return rc;
+    if ((rc = d2h(out->fc_diff, p->d_fcdiff, n, st))) return rc;
+    if ((rc = d2h(out->fcd_ks, p->d_ks, n, st))) return rc;
+    if ((rc = d2h(out->w_ie, p->d_wIE_out, (size_t)n * N, st))) return rc;
+    if ((rc = d2h(out->fic_failed, p->d_failed, n, st))) return rc;
+    if ((rc = d2h(out->fic_ntrials, p->d_trials, n, st))) return rc;
+    if ((rc = d2h(out->fic_unstable, p->d_unstable, n, st))) return rc;
+    if ((rc = d2h(out->ext_means, p->d_ext, (size_t)n * 6 * N, st))) return rc;
+    if (out->bold) {
+        if (c.precision == BNM_PREC_F64)
+            rc = d2h(out->bold, p->d_bold64, (size_t)n * s.frames * N, st);
+        else
+            rc = f2d(out->bold, p->d_bold, (size_t)n * s.frames * N, st);
+        if (rc) return rc;
+    }
+    if ((rc = f2d(out->fc, p->d_fc, (size_t)n * s.n_pairs, st))) return rc;
+    if (!c.no_fcd && (rc = f2d(out->fcd, p->d_fcd, (size_t)n * s.n_fcd, st))) return rc;
+    BNM_CUDA_TRY(cudaStreamSynchronize(st));
+    float ms;
+    for (int i = 0; i < 5; i++) {
+        BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]));
+        p->timings[i] = ms;
+    }
+    BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->ev[0], p->ev[5]));
+    p->timings[5] = ms;
+    if (status & kStatusTimeout) return fail(BNM_ETIMEOUT, "a device wait gave up (status %d)", status);
+    if (status) return fail(BNM_ECUDA, "device status %d", status);
+    return BNM_OK;
+}
+
+extern "C" int bnm_last_timings(bnm_plan* p, double* ms6) {
+    if (!p || !ms6) return fail(BNM_EINVAL, "null argument");
+    for (int i = 0; i < 6; i++) ms6[i] = p->timings[i];
+    return BNM_OK;
+}
+
+extern "C" int bnm_plan_noise(bnm_plan* p, int64_t offset, int64_t n, float* out) {
+    if (!p || !out || offset < 0 || n < 0 || offset + n > p->sz.noise_len) return fail(BNM_EINVAL, "bad noise range");
+    BNM_CUDA_TRY(cudaSetDevice(p->cfg.device));
+    BNM_CUDA_TRY(cudaMemcpy(out, p->d_noise + offset, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    return BNM_OK;
+}
+
+extern "C" int bnm_run_simulations(double* corr, double* fic_penalties, const double* G_list, const double* w_EE_list,
+                                   const double* w_EI_list, const double* w_IE_list, double* w_IE_fic,
+                                   const double* SC, int32_t nodes, int32_t calculate_fic_penalty, int32_t time_steps,
+                                   int32_t BOLD_TR, int32_t max_fic_trials, int32_t sim_only,
+                                   const double* emp_FC_tril, int32_t n_emp_fc, const double* emp_FCD_tril,
+                                   int32_t n_emp_fcd, int32_t window_size, int32_t window_step, int32_t N_SIMS,
+                                   const float* noise, int32_t rand_seed, int32_t do_fic, int32_t adjust_fic,
+                                   int32_t* FIC_failed, int32_t* fic_n_trials, double* BOLD_ex, double* ext_means) {
+    bnm_config cfg;
+    bnm_config_default(&cfg);
+    bnm_config_from_env(&cfg);
+    cfg.nodes = nodes;
+    cfg.max_sims = N_SIMS;
+    cfg.time_steps = time_steps;
+    cfg.bold_tr = BOLD_TR;
+    cfg.window_size = window_size;
+    cfg.window_step = window_step;
+    cfg.max_fic_trials = max_fic_trials;
+    cfg.calculate_fic_penalty = calculate_fic_penalty;
+    cfg.do_fic = do_fic;
+    cfg.numerical_fic = adjust_fic;
+    cfg.noise_mode = noise ? BNM_NOISE_HOST : BNM_NOISE_PHILOX;
+    cfg.noise_seed = (uint64_t)rand_seed;
+    bnm_sizes sz;
+    int rc = bnm_config_sizes(&cfg, &sz);
+    if (rc) return rc;
+    bnm_plan* p = nullptr;
+    rc = bnm_plan_create(&cfg, SC, emp_FC_tril, n_emp_fc, emp_FCD_tril, n_emp_fcd, noise, noise ? sz.noise_len : 0, &p);
+    if (rc) return rc;
+    std::vector<double> cost(N_SIMS), wie_out((size_t)N_SIMS * nodes);
+    bnm_batch_out o;
+    std::memset(&o, 0, sizeof o);
+    o.cost = cost.data();
+    o.fic_penalty = fic_penalties;
+    o.w_ie = wie_out.data();
+    o.fic_failed = FIC_failed;
+    o.fic_ntrials = fic_n_trials;
+    o.bold = BOLD_ex;
+    o.ext_means = ext_means;
+    const double* wie_in = do_fic ? w_IE_fic : w_IE_list;
+    rc = bnm_run(p, N_SIMS, G_list, w_EE_list, w_EI_list, wie_in, &o);
+    bnm_plan_destroy(p);
+    if (rc) return rc;
+    for (int i = 0; i < N_SIMS; i++) corr[i] = sim_only ? cfg.max_cost : cost[i];
+    if (do_fic && w_IE_fic) std::copy(wie_out.begin(), wie_out.end(), w_IE_fic);
+    return BNM_OK;
+}

@@ -1,0 +1,235 @@
+// Analytic FIC initialisation on the device and the Philox noise table.
+//
+// Analytic FIC (reference fic.cpp:130-207, called per particle on the host at
+// run_CMAES.cpp:144-174 by the GPU build and inside bnm() by the CPU build):
+// for every node, solve the inhibitory steady state
+//     I = I0_I + wEI*S_E_ss - w_II*gamma_I*tau_I*phi_I(I)        on [0, 2]
+// with Brent's method (Brent 1973, ch. 4: bracketing, inverse quadratic /
+// secant steps, bisection fallback), stopping when the bracket passes the
+// relative interval test |hi-lo| < 0.001*min(|lo|,|hi|) (fic.cpp:71-100:
+// test_interval(lo, hi, 0, 0.001), at most 100 iterations).  Then
+//     S_I = phi_I(I)*tau_I*gamma_I,
+//     wIE = -(1/S_I) * (I_E_ss - I_ext - I0_E - (G*J_NMDA*SC[j,:] + wEE_j e_j) . S_E_ss).
+// A failed solve or a negative wIE marks the particle unstable, and its wIE is
+// then 1 on every node (run_CMAES.cpp:162-166).  One CTA per particle, one
+// thread per node, FP64 throughout.
+//
+// Noise table: the reference draws standard normals in (ms, substep, node,
+// E|I) order, one stream shared by every particle and every FIC trial
+// (run_CMAES.cpp:640-657, bnm.cpp:187-188, 273-274).  The Philox mode keeps
+// those semantics with a counter-based generator: element e of the table is
+// a function of (seed, e) only.  Philox4x32-10 (Salmon et al., SC'11,
+// "Parallel random numbers: as easy as 1, 2, 3") maps counter e/4 to four
+// 32-bit words, turned into four normals by the Box-Muller transform.
+#include <cstdint>
+#include <cuda_runtime.h>
+#include "kernels.h"
+
+namespace bnm {
+
+
+template <typename R>
+struct FicModel {
+    __device__ static double phi_I(double II) {
+        typedef Model<R> C;
+        return ((C::a_I * II) - C::b_I) / (1 - exp(-1 * C::d_I * ((C::a_I * II) - C::b_I)));
+    }
+};
+
+// Brent zeroin state with the documented GSL iterate/bracket interface.
+struct Brent {
+    double a, b, c, fa, fb, fc, d, e, lo, hi, root;
+};
+
+template <typename R>
+__device__ double inh_curr(double x, double I0_I, double wEI) {
+    const double S_E_ss = 0.1647572075, w_II = (double)Model<R>::w_II, gamma_I_s = 1.0, tau_I_s = 0.01;
+    return I0_I + wEI * S_E_ss - w_II * gamma_I_s * tau_I_s * FicModel<R>::phi_I(x) - x;
+}
+
+template <typename R>
+__device__ bool brent_step(Brent& s, double I0_I, double wEI) {
+    double a = s.a, b = s.b, c = s.c, fa = s.fa, fb = s.fb, fc = s.fc, d = s.d, e = s.e;
+    if ((fb > 0.0 && fc > 0.0) || (fb < 0.0 && fc < 0.0)) {
+        c = a;
+        fc = fa;
+        d = e = b - a;
+    }
+    if (fabs(fc) < fabs(fb)) {
+        a = b; fa = fb;
+        b = c; fb = fc;
+        c = a; fc = fa;
+    }
+    const double tol = 2.0 * 2.220446049250313e-16 * fabs(b);
+    const double m = 0.5 * (c - b);
+    if (fb == 0.0 || fabs(m) <= tol) {
+        s.a = a; s.b = b; s.c = c; s.fa = fa; s.fb = fb; s.fc = fc; s.d = d; s.e = e;
+        s.root = b;
+        s.lo = (b < c) ? b : c;
+        s.hi = (b < c) ? c : b;
+        if (fb == 0.0) s.lo = s.hi = b;
+        return true;
+    }
+    if (fabs(e) >= tol && fabs(fa) > fabs(fb)) {
+        double p, q, r, sr = fb / fa;
+        if (a == c) {
+            p = 2.0 * m * sr;
+            q = 1.0 - sr;
+        } else {
+            q = fa / fc;
+            r = fb / fc;
+            p = sr * (2.0 * m * q * (q - r) - (b - a) * (r - 1.0));
+            q = (q - 1.0) * (r - 1.0) * (sr - 1.0);
+        }
+        if (p > 0.0) q = -q; else p = -p;
+        const double lim1 = 3.0 * m * q - fabs(tol * q), lim2 = fabs(e * q);
+        if (2.0 * p < (lim1 < lim2 ? lim1 : lim2)) {
+            e = d;
+            d = p / q;
+        } else {
+            d = m;
+            e = m;
+        }
+    } else {
+        d = m;
+        e = m;
+    }
+    a = b;
+    fa = fb;
+    b += (fabs(d) > tol) ? d : (m > 0.0 ? tol : -tol);
+    fb = inh_curr<R>(b, I0_I, wEI);
+    if (!isfinite(fb)) return false;
+    s.a = a; s.b = b; s.c = c; s.fa = fa; s.fb = fb; s.fc = fc; s.d = d; s.e = e;
+    s.root = b;
+    double cc = c;
+    if ((fb > 0.0 && fc > 0.0) || (fb < 0.0 && fc < 0.0)) cc = a;
+    s.lo = (b < cc) ? b : cc;
+    s.hi = (b < cc) ? cc : b;
+    return true;
+}
+
+// fic.cpp:26-55: -1 when the interval test does not pass within 100 steps.
+template <typename R>
+__device__ double solve_inh(double I0_I, double wEI) {
+    Brent s;
+    s.a = 0.0;
+    s.b = 2.0;
+    s.fa = inh_curr<R>(0.0, I0_I, wEI);
+    s.fb = inh_curr<R>(2.0, I0_I, wEI);
+    s.c = s.a;
+    s.fc = s.fa;
+    s.d = s.e = 2.0;
+    s.root = 1.0;
+    int iter = 0;
+    bool ok = false;
+    do {
+        iter++;
+        if (!brent_step<R>(s, I0_I, wEI)) break;
+        const double lo = s.lo, hi = s.hi;
+        const double min_abs = ((lo > 0.0 && hi > 0.0) || (lo < 0.0 && hi < 0.0)) ? fmin(fabs(lo), fabs(hi)) : 0.0;
+        ok = fabs(hi - lo) < 0.001 * min_abs;
+    } while (!ok && iter < 100);
+    return ok ? s.root : -1.0;
+}
+
+template <typename R>
+__global__ void analytic_fic_kernel(FicArgs a) {
+    typedef Model<R> C;
+    const int sim = blockIdx.x, N = a.N;
+    __shared__ int s_bad;
+    if (threadIdx.x == 0) s_bad = 0;
+    __syncthreads();
+    const double I0 = (double)C::I_0;
+    const double I0_E = I0 * (double)C::w_E, I0_I = I0 * (double)C::w_I;
+    const double GJ = a.G[sim] * C::J_NMDA;
+    for (int j = threadIdx.x; j < N; j += blockDim.x) {
+        const double wEI = a.wEI[(size_t)sim * N + j], wEE = a.wEE[(size_t)sim * N + j];
+        const double II = solve_inh<R>(I0_I, wEI);
+        bool bad = (II == -1.0);
+        double J = 1.0;
+        if (!bad) {
+            const double SI = FicModel<R>::phi_I(II) * 0.01 * 1.0;
+            double dot = 0.0;
+            const double* row = a.sc + (size_t)j * N;
+            for (int k = 0; k < N; k++) {
+                double kee = row[k] * GJ;
+                if (k == j) kee += wEE;
+                dot += kee * 0.1647572075;
+            }
+            J = (-1 / SI) * (0.3773805650 - (double)C::I_ext - I0_E - dot);
+            bad = J < 0;
+        }
+        if (bad) atomicOr(&s_bad, 1);
+        a.wIE[(size_t)sim * N + j] = J;
+    }
+    __syncthreads();
+    if (s_bad)
+        for (int j = threadIdx.x; j < N; j += blockDim.x) a.wIE[(size_t)sim * N + j] = 1.0;
+    if (threadIdx.x == 0) a.unstable[sim] = s_bad;
+}
+
+// ------------------------------------------------------------- Philox
+__device__ __forceinline__ void philox_round(uint32_t (&c)[4], uint32_t k0, uint32_t k1) {
+    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+    const uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
+    const uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
+    const uint32_t n0 = hi1 ^ c[1] ^ k0, n1 = lo1, n2 = hi0 ^ c[3] ^ k1, n3 = lo0;
+    c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
+}
+
+__device__ __forceinline__ void philox4x32_10(uint32_t (&c)[4], uint32_t k0, uint32_t k1) {
+#pragma unroll
+    for (int r = 0; r < 10; r++) {
+        philox_round(c, k0, k1);
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+}
+
+// Four standard normals for counter `ctr` (table elements 4*ctr .. 4*ctr+3).
+__device__ __forceinline__ float4 philox_normals(uint64_t seed, uint64_t ctr) {
+    uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), 0u, 0u};
+    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
+    const float s = 2.3283064365386963e-10f;  // 2^-32
+    // uniforms in (0, 1]
+    const float u0 = ((float)c[0] + 1.0f) * s, u1 = ((float)c[1] + 0.5f) * s;
+    const float u2 = ((float)c[2] + 1.0f) * s, u3 = ((float)c[3] + 0.5f) * s;
+    const float r0 = sqrtf(-2.0f * logf(fminf(u0, 1.0f))), r1 = sqrtf(-2.0f * logf(fminf(u2, 1.0f)));
+    float s0, c0, s1, c1;
+    sincospif(2.0f * u1, &s0, &c0);
+    sincospif(2.0f * u3, &s1, &c1);
+    return make_float4(r0 * c0, r0 * s0, r1 * c1, r1 * s1);
+}
+
+__global__ void philox_fill_kernel(float* out, uint64_t n, uint64_t seed) {
+    const uint64_t n4 = (n + 3) / 4;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * blockDim.x) {
+        const float4 v = philox_normals(seed, i);
+        const uint64_t e = 4 * i;
+        if (e + 3 < n) {
+            reinterpret_cast<float4*>(out)[i] = v;
+        } else {
+            if (e < n) out[e] = v.x;
+            if (e + 1 < n) out[e + 1] = v.y;
+            if (e + 2 < n) out[e + 2] = v.z;
+        }
+    }
+}
+
+}  // namespace bnm
+
+using namespace bnm;
+
+cudaError_t bnm_launch_analytic_fic(const FicArgs& a, cudaStream_t st) {
+    const int threads = a.N < 256 ? ((a.N + 31) / 32) * 32 : 256;
+    if (a.fp32_consts)
+        analytic_fic_kernel<float><<<a.n_sims, threads, 0, st>>>(a);
+    else
+        analytic_fic_kernel<double><<<a.n_sims, threads, 0, st>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t bnm_launch_philox(float* out, uint64_t n, uint64_t seed, int num_sms, cudaStream_t st) {
+    philox_fill_kernel<<<num_sms * 8, 256, 0, st>>>(out, n, seed);
+    return cudaGetLastError();
+}

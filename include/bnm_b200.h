@@ -1,0 +1,200 @@
+/*
+ * bnm_b200 -- C ABI of the B200 simulate-and-fit library.
+ *
+ * Drop-in boundary for the reference's batch entry point and its driver
+ * (amnsbr/bnm_cuda):
+ *
+ *   run_simulations(...)        bnm.cu:594-617   (GPU build; called per CMA-ES
+ *                               generation at run_CMAES.cpp:758-780 and for the
+ *                               best-particle rerun at run_CMAES.cpp:875-897)
+ *                               bnm.cpp:431-439  (CPU build, same meaning)
+ *   analytical_fic(...)         fic.cpp:130-207  (per particle, run_CMAES.cpp:144-174)
+ *   noise precompute            run_CMAES.cpp:640-657
+ *   CMAES_Points()              cmaes.cpp:128-557 (driven at run_CMAES.cpp:714-818)
+ *   BNM_* runtime configuration constants.h:93-116
+ *
+ * All signatures use plain C types.  Every entry point returns a status
+ * (BNM_OK or a BNM_E* code) instead of exiting the process; bnm_last_error()
+ * gives the message.  Host arrays are flat, particle-major ([n][nodes]).
+ */
+#ifndef BNM_B200_H
+#define BNM_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BNM_OK 0
+#define BNM_EINVAL 1   /* bad argument or size (the reference exits in these cases) */
+#define BNM_ENOMEM 2   /* device allocation failed */
+#define BNM_ECUDA 3    /* CUDA runtime error */
+#define BNM_ETIMEOUT 4 /* a bounded device wait gave up */
+
+/* Arithmetic of the integrator.  FP32 is the product path (FP32 integration,
+ * FP64 FIC solve and FP64 centring of BOLD / window series).  F64 and F32_REF
+ * are the reference-order kernels (no FMA contraction): F64 follows the
+ * reference's default double build, F32_REF its USE_FLOATS build. */
+enum { BNM_PREC_F32 = 0, BNM_PREC_F64 = 1, BNM_PREC_F32_REF = 2 };
+
+/* Noise source.  PHILOX: counter-based table keyed by noise_seed, shared by
+ * all particles and FIC trials (the reference's common-random-numbers
+ * semantics).  HOST: the caller's precomputed table (the reference's
+ * mt19937 + normal_distribution<float> stream, run_CMAES.cpp:640-657). */
+enum { BNM_NOISE_PHILOX = 0, BNM_NOISE_HOST = 1 };
+
+/* Run configuration: the reference's CLI arguments and BNM_* settings. */
+typedef struct bnm_config {
+    int32_t nodes;             /* argv[6] */
+    int32_t max_sims;          /* particles per call (lambda, argv[17]) */
+    int32_t time_steps;        /* argv[12], ms; the loop runs 0..time_steps */
+    int32_t bold_tr;           /* argv[13], ms */
+    int32_t window_step;       /* argv[14] */
+    int32_t window_size;       /* argv[15] */
+    int32_t bold_remove_s;     /* BNM_BOLD_REMOVE (30) */
+    int32_t exc_interhem;      /* BNM_EXC_INTERHEM (1) */
+    int32_t do_fic;            /* wIE from FIC (argv[10] == 0) */
+    int32_t numerical_fic;     /* BNM_NUMERICAL_FIC (1) */
+    int32_t max_fic_trials;    /* BNM_MAX_FIC_TRIALS_CMAES (10) */
+    int32_t i_sampling_start;  /* BNM_I_SAMPLING_START (1000) */
+    int32_t i_sampling_end;    /* BNM_I_SAMPLING_END (10000) */
+    double init_delta;         /* BNM_INIT_DELTA (0.02, rounded to float as the reference does) */
+    int32_t use_fc_diff;       /* BNM_USE_FC_DIFF (1) */
+    int32_t fic_reject_failed; /* BNM_CMAES_FIC_REJECT_FAILED (0) */
+    double fic_penalty_scale;  /* BNM_CMAES_FIC_PENALTY_SCALE (2) */
+    double max_cost;           /* BNM_MAX_COST (2) */
+    int32_t calculate_fic_penalty; /* on when do_fic (run_CMAES.cpp:389) */
+    int32_t no_fcd;            /* fcd path "no_fcd" (run_CMAES.cpp:331) */
+    int32_t precision;         /* BNM_PREC_* */
+    int32_t noise_mode;        /* BNM_NOISE_* */
+    uint64_t noise_seed;       /* argv[16] */
+    int32_t device;
+} bnm_config;
+
+/* Reference defaults (constants.h:93-116). */
+void bnm_config_default(bnm_config *cfg);
+/* Overlay the BNM_* environment variables the way the reference reads them
+ * (doubles pass through float, helpers.cpp:4-11). */
+void bnm_config_from_env(bnm_config *cfg);
+
+const char *bnm_last_error(void);
+int bnm_device_count(void);
+
+/* Derived sizes of a configuration (no device work). */
+typedef struct bnm_sizes {
+    int32_t frames;        /* BOLD frames, time_steps / bold_tr + 1 (run_CMAES.cpp:476-477) */
+    int32_t n_vols_remove; /* bold_remove_s * 1000 / bold_tr (run_CMAES.cpp:483) */
+    int32_t corr_len;      /* frames - n_vols_remove */
+    int32_t n_pairs;       /* FC lower-triangle length (run_CMAES.cpp:494-500) */
+    int32_t n_windows;     /* FCD windows (run_CMAES.cpp:531-556) */
+    int32_t window_len;    /* frames per window */
+    int32_t n_fcd;         /* n_windows * (n_windows - 1) / 2 */
+    int64_t noise_len;     /* nodes * (time_steps + 1) * 10 * 2 floats */
+} bnm_sizes;
+int bnm_config_sizes(const bnm_config *cfg, bnm_sizes *out);
+
+/* ------------------------------------------------------------------ plans
+ * A plan owns every device buffer of a configuration (SC, targets, noise
+ * table, per-particle work space for max_sims particles) so that one call per
+ * CMA-ES generation allocates nothing.  One plan per thread at a time. */
+typedef struct bnm_plan bnm_plan;
+
+/* sc: nodes*nodes row-major.  emp_fc: n_pairs values in the reference's pair
+ * order.  emp_fcd: any length > 0 (unless no_fcd).  host_noise: required for
+ * BNM_NOISE_HOST, noise_len floats. */
+int bnm_plan_create(const bnm_config *cfg, const double *sc, const double *emp_fc, int32_t n_emp_fc,
+                    const double *emp_fcd, int32_t n_emp_fcd, const float *host_noise, int64_t n_host_noise,
+                    bnm_plan **out);
+void bnm_plan_destroy(bnm_plan *plan);
+
+/* Per-particle outputs; every pointer except cost may be NULL. */
+typedef struct bnm_batch_out {
+    double *cost;        /* [n] 1 - r(FC) + KS(FCD) (+ |dmean FC|); max_cost on NaN.  = corr[] of run_simulations */
+    double *fic_penalty; /* [n] (0 when not calculated) */
+    double *fc_corr;     /* [n] */
+    double *fc_diff;     /* [n] */
+    double *fcd_ks;      /* [n] */
+    double *w_ie;        /* [n][nodes] wIE after FIC (the reference's w_IE_fic out) */
+    int32_t *fic_failed; /* [n] */
+    int32_t *fic_ntrials;/* [n] */
+    int32_t *fic_unstable; /* [n] analytic FIC was unstable (wIE set to 1) */
+    double *ext_means;   /* [n][6][nodes] S_E, I_E, r_E, S_I, I_I, r_I means over kept frames */
+    double *bold;        /* [n][frames][nodes] */
+    double *fc;          /* [n][n_pairs] */
+    double *fcd;         /* [n][n_fcd] */
+} bnm_batch_out;
+
+/* One batch (a CMA-ES generation): integrate, BOLD, FC, window FC, FCD, KS,
+ * goodness of fit and FIC penalty for n <= max_sims particles.
+ * G [n]; w_ee, w_ei [n][nodes].  w_ie [n][nodes]: the fixed wIE when
+ * do_fic == 0; with do_fic it is the analytic-FIC starting point (as the
+ * reference GPU driver's w_IE_fic), or NULL to compute it on the device. */
+int bnm_run(bnm_plan *plan, int32_t n, const double *G, const double *w_ee, const double *w_ei, const double *w_ie,
+            bnm_batch_out *out);
+
+/* Analytic FIC alone (fic.cpp:130-207) for n particles on the device. */
+int bnm_analytic_fic(bnm_plan *plan, int32_t n, const double *G, const double *w_ee, const double *w_ei,
+                     double *w_ie_out, int32_t *unstable_out);
+
+/* Time of the last bnm_run on the device, per stage, in ms:
+ * [0] analytic FIC, [1] integration, [2] FC + window FC, [3] FCD + KS histogram, [4] GOF, [5] total. */
+int bnm_last_timings(bnm_plan *plan, double *ms6);
+
+/* Device noise table of the plan, copied out (n floats from offset). */
+int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);
+
+/* ------------------------------------------------------ one-shot mirror
+ * Same argument meaning as the reference's run_simulations (bnm.cu:594-617),
+ * flattened: builds a plan, runs one batch, releases it.  corr receives the
+ * goodness-of-fit cost, fic_penalties the FIC penalty, w_IE_fic (in/out, may
+ * be NULL) the FIC weights, FIC_failed / fic_n_trials the numerical FIC
+ * outcome, BOLD_ex the BOLD frames ([N_SIMS][output_ts][nodes], may be NULL),
+ * ext_means the extended outputs (may be NULL).  noise may be NULL (Philox,
+ * seeded by rand_seed). */
+int bnm_run_simulations(double *corr, double *fic_penalties, const double *G_list, const double *w_EE_list,
+                        const double *w_EI_list, const double *w_IE_list, double *w_IE_fic, const double *SC,
+                        int32_t nodes, int32_t calculate_fic_penalty, int32_t time_steps, int32_t BOLD_TR,
+                        int32_t max_fic_trials, int32_t sim_only, const double *emp_FC_tril, int32_t n_emp_fc,
+                        const double *emp_FCD_tril, int32_t n_emp_fcd, int32_t window_size, int32_t window_step,
+                        int32_t N_SIMS, const float *noise, int32_t rand_seed, int32_t do_fic, int32_t adjust_fic,
+                        int32_t *FIC_failed, int32_t *fic_n_trials, double *BOLD_ex, double *ext_means);
+
+/* ------------------------------------------------------------- CMA-ES
+ * Host optimiser with the semantics of the reference's CMAES_Points
+ * (cmaes.cpp:128-557): Hansen's CMA-ES (2006 "Variante 6" or 2016 "16"),
+ * coordinates in [0,1], boundary penalty (Hansen et al. 2009), early stop on
+ * a flat best-cost history.  Random streams as in the reference
+ * (std::default_random_engine seeded SeedMW and 11+it). */
+typedef struct bnm_cmaes bnm_cmaes;
+typedef struct bnm_cmaes_params {
+    int32_t lambda, dimension, seed_mw, it_max;
+    int32_t variante;       /* BNM_CMAES_VARIANTE (6) */
+    double sigma;           /* BNM_CMAES_SIGMA (0.5) */
+    double alphacov;        /* BNM_CMAES_ALPHACOV (2) */
+    double gamma_scale;     /* BNM_CMAES_GAMMA_SCALE (2) */
+    double bound_soft_edge; /* BNM_CMAES_BOUND_SOFT_EDGE (0) */
+    int32_t early_stop_gens;/* BNM_CMAES_EARLY_STOP_GENS (30) */
+    double early_stop_tol;  /* BNM_CMAES_EARLY_STOP_TOL (1e-3) */
+} bnm_cmaes_params;
+void bnm_cmaes_params_default(bnm_cmaes_params *p);
+void bnm_cmaes_params_from_env(bnm_cmaes_params *p);
+/* Creates the optimiser and samples generation 0 (the first CMAES_Points call). */
+int bnm_cmaes_create(const bnm_cmaes_params *p, bnm_cmaes **out);
+void bnm_cmaes_destroy(bnm_cmaes *c);
+/* Iteration counter (the reference's global `it`); >= it_max means stop. */
+int32_t bnm_cmaes_iteration(const bnm_cmaes *c);
+/* Current sample points: feasible [dim][lambda] (clipped to [0,1]), raw and preferred (may be NULL). */
+int bnm_cmaes_samples(const bnm_cmaes *c, double *feasible, double *raw, double *preferred);
+/* Report the costs of the current samples (gof cost + FIC penalty, lower is
+ * better); computes the boundary penalty (written to penalized, may be NULL)
+ * and samples the next generation.  Returns the new iteration counter. */
+int32_t bnm_cmaes_tell(bnm_cmaes *c, const double *cost, double *penalized);
+/* Best feasible point [dim] and its value (-cost, the reference's CBVfeas[D]). */
+int bnm_cmaes_best(const bnm_cmaes *c, double *x, double *value);
+int bnm_cmaes_state(const bnm_cmaes *c, double *mean, double *sigma, double *C);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

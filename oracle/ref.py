@@ -1,0 +1,254 @@
+"""TEST INFRASTRUCTURE ONLY (oracle): ctypes access to
+
+* ``_ref/libbnmref_{f64,f32}.so`` -- the reference's own CPU sources
+  (bnm.cpp, check_fit.cpp, fic.cpp, cmaes.cpp) compiled unmodified against the
+  GSL/libks stand-ins in ``compat/`` (see Makefile), and
+* ``libbnm_port.so`` -- this project's CPU restatement of the same path
+  (bnm_port.cpp), which the tests pin against the reference build and then
+  use to check the CUDA path.
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU-baseline leg may
+import this module.  The reference reads its ``BNM_*`` configuration from the
+environment when the library is loaded (constants.h:93-116), so callers that
+need another configuration run in a fresh process (``run_isolated``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_libs: dict = {}
+
+dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+
+
+def ref_available(fp32: bool = False) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libbnmref_{'f32' if fp32 else 'f64'}.so"))
+
+
+def port_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "libbnm_port.so"))
+
+
+def _d(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def ref_lib(fp32: bool = False):
+    key = "f32" if fp32 else "f64"
+    if key not in _libs:
+        lib = C.CDLL(os.path.join(HERE, "_ref", f"libbnmref_{key}.so"))
+        lib.ref_run_simulations.argtypes = [dp, dp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_int, dp, C.c_int, dp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_char_p, C.c_int, C.c_int, C.c_int]
+        lib.ref_fc_tril.argtypes = [dp, C.c_int, C.c_int, C.c_int, dp]
+        lib.ref_fcd_tril.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, C.c_int]
+        lib.ref_check_fit_bold.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, C.c_int,
+                                           C.c_int, C.c_int]
+        lib.ref_check_fit_bold.restype = C.c_double
+        lib.ref_ks_stat.argtypes = [dp, C.c_int, dp, C.c_int]
+        lib.ref_ks_stat.restype = C.c_double
+        lib.ref_analytical_fic.argtypes = [dp, C.c_int, C.c_double, dp, dp, dp]
+        lib.ref_constants.argtypes = [dp]
+        lib.ref_cmaes_setup.argtypes = [C.c_int] * 4
+        lib.ref_cmaes_get.argtypes = [dp, dp, dp]
+        lib.ref_cmaes_tell.argtypes = [dp, dp]
+        lib.ref_cmaes_best.argtypes = [dp]
+        lib.ref_cmaes_state.argtypes = [dp, dp, dp]
+        _libs[key] = lib
+    return _libs[key]
+
+
+def port_lib():
+    if "port" not in _libs:
+        lib = C.CDLL(os.path.join(HERE, "libbnm_port.so"))
+        lib.port_noise.argtypes = [C.c_int, C.c_int64, fp]
+        lib.port_analytic_fic.argtypes = [C.c_int, dp, C.c_int, C.c_double, dp, dp, dp]
+        integ = [dp, C.c_int, C.c_double, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p,
+                 C.c_int, C.c_int, C.c_double, dp, dp, C.POINTER(C.c_int), C.POINTER(C.c_int), dp]
+        lib.port_integrate_f64.argtypes = integ
+        lib.port_integrate_f32.argtypes = integ
+        lib.port_fic_penalty.argtypes = [C.c_int, dp, C.c_int, C.c_double, C.c_int, C.c_int]
+        lib.port_fic_penalty.restype = C.c_double
+        lib.port_fc_tril.argtypes = [dp, C.c_int, C.c_int, C.c_int, dp]
+        lib.port_windows.argtypes = [C.c_int, C.c_int, C.c_int, ip, ip, C.c_int]
+        lib.port_fcd_tril.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, C.c_void_p]
+        lib.port_gof.argtypes = [dp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, C.c_int, C.c_int,
+                                 C.c_double, dp]
+        lib.port_ks.argtypes = [dp, C.c_int, dp, C.c_int]
+        lib.port_ks.restype = C.c_double
+        lib.port_run_batch.argtypes = [C.c_int, C.c_int, dp, C.c_int, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int,
+                                       C.c_int, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double,
+                                       C.c_int, C.c_int, C.c_int, dp, C.c_int, dp, C.c_int, C.c_int, C.c_double,
+                                       C.c_double, C.c_int, C.c_int, dp, dp, dp, ip, ip]
+        _libs["port"] = lib
+    return _libs["port"]
+
+
+# --------------------------------------------------------------- reference
+def ref_constants(fp32=False) -> dict:
+    out = np.zeros(15)
+    ref_lib(fp32).ref_constants(out)
+    keys = ["bold_remove_s", "max_cost", "i_sampling_start", "i_sampling_end", "i_sampling_duration",
+            "numerical_fic", "max_fic_trials_cmaes", "init_delta", "use_fc_diff", "exc_interhem",
+            "fic_penalty_scale", "fic_reject_failed", "sigma", "early_stop_gens", "early_stop_tol"]
+    return dict(zip(keys, out.tolist()))
+
+
+def ref_run_simulations(SC, G, wEE, wEI, wIE, *, time_steps, bold_tr, rand_seed, max_fic_trials, emp_fc, emp_fcd,
+                        window_step, window_size, calculate_fic_penalty=True, sim_only=False, no_fcd=False,
+                        out_prefix="", save_output=False, extended_output=False, fp32=False):
+    """run_simulations of bnm.cpp:431-466.  Returns (cost[n], fic_penalty[n])."""
+    n, N = len(G), SC.shape[0]
+    cost, pen = np.zeros(n), np.zeros(n)
+    emp_fcd = _d(emp_fcd) if emp_fcd is not None and len(emp_fcd) else np.zeros(1)
+    ref_lib(fp32).ref_run_simulations(cost, pen, _d(G), _d(wEE).ravel(), _d(wEI).ravel(), _d(wIE).ravel(), _d(SC),
+                                      N, n, int(calculate_fic_penalty), time_steps, bold_tr, rand_seed,
+                                      max_fic_trials, _d(emp_fc), len(emp_fc), emp_fcd, len(emp_fcd), int(sim_only),
+                                      int(no_fcd), window_step, window_size, out_prefix.encode(), 0,
+                                      int(save_output), int(extended_output))
+    return cost, pen
+
+
+def ref_fc_tril(bold, exc=True, fp32=False):
+    bold = _d(bold)
+    T, N = bold.shape
+    out = np.zeros(N * N)
+    n = ref_lib(fp32).ref_fc_tril(bold, T, N, int(exc), out)
+    return None if n < 0 else out[:n]
+
+
+def ref_fcd_tril(bold, step, window_size, exc=True, drop_edges=True, fp32=False):
+    bold = _d(bold)
+    T, N = bold.shape
+    cap = T * T
+    out = np.zeros(cap)
+    n = ref_lib(fp32).ref_fcd_tril(bold, T, N, step, window_size, int(drop_edges), int(exc), out, cap)
+    return None if n < 0 else out[:n]
+
+
+def ref_check_fit_bold(bold, step, window_size, emp_fc, emp_fcd, exc=True, no_fcd=False, fp32=False):
+    bold = _d(bold)
+    T, N = bold.shape
+    return ref_lib(fp32).ref_check_fit_bold(bold, T, N, step, window_size, 1, _d(emp_fc), len(emp_fc), _d(emp_fcd),
+                                            len(emp_fcd), int(no_fcd), int(exc))
+
+
+def ref_analytical_fic(SC, G, wEE, wEI, fp32=False):
+    N = SC.shape[0]
+    out = np.zeros(N)
+    unstable = ref_lib(fp32).ref_analytical_fic(_d(SC), N, float(G), _d(wEE), _d(wEI), out)
+    return out, bool(unstable)
+
+
+# -------------------------------------------------------------------- port
+def port_noise(seed: int, n: int) -> np.ndarray:
+    out = np.zeros(n, dtype=np.float32)
+    port_lib().port_noise(seed, n, out)
+    return out
+
+
+def port_analytic_fic(SC, G, wEE, wEI, fp32=False):
+    N = SC.shape[0]
+    out = np.zeros(N)
+    u = port_lib().port_analytic_fic(int(fp32), _d(SC), N, float(G), _d(wEE), _d(wEI), out)
+    return out, bool(u)
+
+
+def port_integrate(SC, G, wEE, wEI, wIE, *, time_steps, bold_tr, n_vols_remove, seed=0, noise=None,
+                   adjust_fic=True, max_fic_trials=10, sampling_start=1000, sampling_end=10000,
+                   init_delta=float(np.float32(0.02)), fp32=False):
+    """One simulation of bnm.cpp:26-290.  Returns dict(bold [frames, N],
+    wIE [N], trials, failed, ext [6, N] = means of S_E, I_E, r_E, S_I, I_I, r_I)."""
+    N = SC.shape[0]
+    frames = time_steps // bold_tr + 1
+    bold, w, ext = np.zeros(frames * N), np.zeros(N), np.zeros(6 * N)
+    tr, fl = C.c_int(0), C.c_int(0)
+    nz = None
+    if noise is not None:
+        noise = np.ascontiguousarray(noise, dtype=np.float32)
+        nz = noise.ctypes.data_as(C.c_void_p)
+    fn = port_lib().port_integrate_f32 if fp32 else port_lib().port_integrate_f64
+    fn(_d(SC), N, float(G), _d(wEE), _d(wEI), _d(wIE), int(adjust_fic), max_fic_trials, time_steps, bold_tr,
+       n_vols_remove, seed, nz, sampling_start, sampling_end, init_delta, bold, w, C.byref(tr), C.byref(fl), ext)
+    return dict(bold=bold.reshape(frames, N), wIE=w, trials=tr.value, failed=fl.value, ext=ext.reshape(6, N))
+
+
+def port_fic_penalty(mean_rE, failed=0, scale=2.0, reject_failed=0, fp32=False):
+    mean_rE = _d(mean_rE)
+    return port_lib().port_fic_penalty(int(fp32), mean_rE, len(mean_rE), scale, reject_failed, int(failed))
+
+
+def port_fc_tril(bold, exc=True):
+    bold = _d(bold)
+    T, N = bold.shape
+    out = np.zeros(N * N)
+    n = port_lib().port_fc_tril(bold, T, N, int(exc), out)
+    return None if n < 0 else out[:n]
+
+
+def port_fcd_tril(bold, step, window_size, exc=True, window_fc=False):
+    bold = _d(bold)
+    T, N = bold.shape
+    out = np.zeros(T * T)
+    P = N * (N - 1) // 2 - ((N // 2) ** 2 if exc else 0)
+    wfc = np.zeros(T * P) if window_fc else None
+    n = port_lib().port_fcd_tril(bold, T, N, step, window_size, int(exc), out,
+                                 wfc.ctypes.data_as(C.c_void_p) if window_fc else None)
+    if n < 0:
+        return None
+    if window_fc:
+        W = int(round((1 + np.sqrt(1 + 8 * n)) / 2))
+        return out[:n], wfc[:W * P].reshape(W, P)
+    return out[:n]
+
+
+def port_gof(bold, step, window_size, emp_fc, emp_fcd, exc=True, use_fc_diff=True, max_cost=2.0):
+    """-> dict(fc_corr, fc_diff, fcd_ks, cost) of check_fit.cpp:138-217."""
+    bold = _d(bold)
+    T, N = bold.shape
+    out = np.zeros(4)
+    port_lib().port_gof(bold, T, N, step, window_size, int(exc), _d(emp_fc), len(emp_fc), _d(emp_fcd), len(emp_fcd),
+                        int(use_fc_diff), max_cost, out)
+    return dict(fc_corr=out[0], fc_diff=out[1], fcd_ks=out[2], cost=out[3])
+
+
+def port_ks(x, y):
+    return port_lib().port_ks(_d(x), len(x), _d(y), len(y))
+
+
+def port_run_batch(SC, G, wEE, wEI, wIE, *, time_steps, bold_tr, n_vols_remove, seed, window_step, window_size,
+                   emp_fc, emp_fcd, noise=None, do_fic=True, adjust_fic=True, max_fic_trials=10, exc=True,
+                   use_fc_diff=True, max_cost=2.0, pen_scale=2.0, reject_failed=0, sampling_start=1000,
+                   sampling_end=10000, init_delta=float(np.float32(0.02)), fp32=False, n_threads=0):
+    """OpenMP batch of port simulations.  -> dict(cost, fic_penalty, wIE, trials, failed)."""
+    n, N = len(G), SC.shape[0]
+    cost, pen, w = np.zeros(n), np.zeros(n), np.zeros(n * N)
+    tr, fl = np.zeros(n, np.int32), np.zeros(n, np.int32)
+    nz = None
+    if noise is not None:
+        noise = np.ascontiguousarray(noise, dtype=np.float32)
+        nz = noise.ctypes.data_as(C.c_void_p)
+    port_lib().port_run_batch(int(fp32), n, _d(SC), N, _d(G), _d(wEE).ravel(), _d(wEI).ravel(), _d(wIE).ravel(),
+                              int(do_fic), int(adjust_fic), max_fic_trials, time_steps, bold_tr, n_vols_remove, seed,
+                              nz, sampling_start, sampling_end, init_delta, window_step, window_size, int(exc),
+                              _d(emp_fc), len(emp_fc), _d(emp_fcd), len(emp_fcd), int(use_fc_diff), max_cost,
+                              pen_scale, reject_failed, n_threads, cost, pen, w, tr, fl)
+    return dict(cost=cost, fic_penalty=pen, wIE=w.reshape(n, N), trials=tr, failed=fl)
+
+
+def run_isolated(fn, *args, env=None, **kwargs):
+    """Run ``fn`` in a fresh spawned process with extra environment (the
+    reference reads BNM_* at load time)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1, initializer=_set_env, initargs=(env or {},)) as pool:
+        return pool.apply(fn, args, kwargs)
+
+
+def _set_env(env):
+    os.environ.update({k: str(v) for k, v in env.items()})
