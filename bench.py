@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the simulate-and-fit hot path: one CMA-ES generation.
+
+Workload (one step): 256 particles sharing one synthetic 100-node connectome
+(30 % density, log-normal weights, max row sum 1, seed 0), each simulated for
+450 s of model time (dt 0.1 ms, 4.5 M Euler-Maruyama substeps) with analytic
++ numerical FIC (up to 10 restarts), Balloon-Windkessel BOLD at TR 0.72 s
+(626 frames, 41 removed), FC (2450 pairs), sliding-window FC (window 44 TRs,
+step 1: 541 windows), FCD (146,070 entries), the KS distance to a target FCD
+and the goodness of fit.  Parameters: G uniform on [0.5, 4], wEE and wEI
+uniform on [0.05, 0.75].  Targets: the model's own FC/FCD at G=2, wEE=0.3,
+wEI=0.2 (synthetic, seeded).  Noise: device Philox table, seed 410.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line.  ``value`` is sims/s from the device-side stage timers
+(CUDA events on the plan's stream) with every input resident in HBM; ``e2e``
+is sims/s through the public C-ABI call (bnm_run) with host buffers: parameter
+upload and result download are inside the timed region.  Under torchrun each
+rank runs its own generation (weak scaling) and the costs are all-gathered,
+as a host CMA-ES needs them; times are the max over ranks.
+
+``--impl reference`` times the reference's own OpenMP CPU path (bnm.cpp
+run_simulations compiled from its sources, oracle/_ref) on every host core,
+on a bounded sample per step: one particle per core simulated for 12 s of
+model time (enough for the FIC sampling window), scaled to full 450 s
+simulations by the substeps executed (FIC restarts included), plus the
+reference's measured FC/FCD/KS cost for one full-size BOLD series.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_NODES, N_SIMS, T_MS, TR, WS, STEP, REMOVE_S = 100, 256, 450_000, 720, 44, 1, 30
+SAMPLE_MS = 12_000
+WORKLOAD = "cmaes-generation-N100-450s-x256"
+
+
+def workload_inputs(rank: int = 0):
+    from bnm_cuda_b200 import synth
+
+    sc = synth.make_sc(N_NODES, 0.3, 0)
+    G, wEE, wEI = synth.uniform_params(N_SIMS, N_NODES, 1 + rank)
+    return sc, G, wEE, wEI
+
+
+def make_targets(sc):
+    """The model's own FC/FCD at G=2, wEE=0.3, wEI=0.2 (device, FP32, Philox seed 1)."""
+    import bnm_cuda_b200 as B
+
+    cfg = B.Config(nodes=N_NODES, max_sims=1, time_steps=T_MS, bold_tr=TR, window_size=WS, window_step=STEP,
+                   bold_remove_s=REMOVE_S, noise_seed=1)
+    s = cfg.sizes()
+    with B.Plan(cfg, sc, np.zeros(s["n_pairs"]), np.zeros(s["n_fcd"])) as p:
+        r = p.run(2.0, 0.3, 0.2, outputs=("fc", "fcd"))
+    return r["fc"][0], r["fcd"][0]
+
+
+class ClockSampler:
+    """nvidia-smi samples (200 ms) of SM clock and throttle reasons."""
+
+    def __init__(self, device: int):
+        self.device, self.proc, self.path = device, None, None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.device}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        try:
+            for line in open(self.path):
+                f = [x.strip() for x in line.split(",")]
+                if len(f) < 9:
+                    continue
+                try:
+                    sm.append(float(f[1]))
+                    mx = max(mx, float(f[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, f[5:9]):
+                    if v.lower().startswith("active"):
+                        reasons.add(n)
+        except OSError:
+            pass
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------ CPU side
+class _QuietStdout:
+    """Silence C-level stdout (the reference prints one line per particle)."""
+
+    def __enter__(self):
+        sys.stdout.flush()
+        self.saved = os.dup(1)
+        devnull = os.open(os.devnull, os.O_WRONLY)
+        os.dup2(devnull, 1)
+        os.close(devnull)
+
+    def __exit__(self, *a):
+        os.dup2(self.saved, 1)
+        os.close(self.saved)
+
+
+_TRIALS = {}
+
+
+def cpu_reference_sample(n_threads: int, sample_ms: int = SAMPLE_MS):
+    """One bounded sample of the reference's CPU run_simulations (see module
+    docstring).  Returns (sims_per_s, detail)."""
+    os.environ.setdefault("OMP_NUM_THREADS", str(n_threads))
+    from oracle import ref
+
+    if not ref.ref_available():
+        return None
+    sc, G, wEE, wEI = workload_inputs(0)
+    idx = np.arange(n_threads) % N_SIMS
+    n = len(idx)
+    zeros = np.zeros((n, N_NODES))
+    emp_fc, emp_fcd = np.zeros(2450), np.zeros(10)
+    fic = sample_ms >= 10_000
+    with _QuietStdout():
+        t0 = time.perf_counter()
+        ref.ref_run_simulations(sc, G[idx], wEE[idx], wEI[idx], zeros if fic else zeros + 1.0, time_steps=sample_ms,
+                                bold_tr=1000, rand_seed=410, max_fic_trials=10, emp_fc=emp_fc, emp_fcd=emp_fcd,
+                                window_step=1, window_size=2, sim_only=True)
+        t_sample = time.perf_counter() - t0
+    if not fic:
+        return None
+    # FIC restarts of these particles (they happen in the first 10 s).  The
+    # reference only reports them in its text output; the port reproduces the
+    # reference bit for bit, so the counts come from it, once per process.
+    key = (n_threads,)
+    if key not in _TRIALS:
+        with _QuietStdout():
+            _TRIALS[key] = ref.port_run_batch(
+                sc, G[idx], wEE[idx], wEI[idx], zeros, time_steps=10_000, bold_tr=1000, n_vols_remove=0, seed=410,
+                window_step=1, window_size=2, emp_fc=np.zeros(20), emp_fcd=np.zeros(10),
+                n_threads=n_threads)["trials"] if ref.port_available() else np.zeros(n)
+    tr = _TRIALS[key]
+    s_sample = 10 * (sample_ms + 1) + 100_000 * tr
+    s_full = 10 * (T_MS + 1) + 100_000 * tr
+    rate = s_sample.max() / t_sample  # substeps per second per core (threads run in parallel)
+    # the reference's FC / FCD / KS on one full-size BOLD series
+    bold = np.random.default_rng(0).standard_normal((626 - 41, N_NODES)) * 0.01
+    t1 = time.perf_counter()
+    with _QuietStdout():
+        ref.ref_check_fit_bold(bold, STEP, WS, np.random.default_rng(2).uniform(-1, 1, 2450),
+                               np.random.default_rng(1).uniform(-1, 1, 1000))
+    t_gof = time.perf_counter() - t1
+    per_sim = s_full.mean() / rate + t_gof
+    sims_per_s = n_threads / per_sim
+    return sims_per_s, {"sample": f"{n} particles x {SAMPLE_MS} ms model time (1 per core, FIC on), scaled by "
+                                  f"substeps to {T_MS} ms + one full FC/FCD/KS ({t_gof:.2f} s)",
+                        "sample_s": t_sample, "per_sim_s": per_sim}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    cores = len(os.sched_getaffinity(0))
+    vals = []
+    from oracle import ref
+
+    if not ref.ref_available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref reference build missing"}))
+        return 0
+    for i in range(args.warmup):  # short, FIC-free warm-up samples
+        cpu_reference_sample(cores, sample_ms=2_000)
+    for i in range(args.steps):
+        r = cpu_reference_sample(cores)
+        vals.append(r[0])
+    v = float(np.mean(vals))
+    print(json.dumps({
+        "impl": "reference", "metric": "sims/s", "value": v, "unit": "sims/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000 * N_SIMS / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD, "nodes": N_NODES, "particles": N_SIMS, "model_time_ms": T_MS,
+                   "tr_ms": TR, "window": WS, "step": STEP},
+        "cpu_baseline": {"value": v, "unit": "sims/s", "cores": cores, "kind": "reference", "sample": r[1]["sample"]},
+        "e2e": {"value": v, "unit": "sims/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+    return 0
+
+
+# ------------------------------------------------------------------ GPU side
+def run_b200(args):
+    import bnm_cuda_b200 as B
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    sc, G, wEE, wEI = workload_inputs(rank)
+    emp_fc, emp_fcd = make_targets(sc)
+    cfg = B.Config(nodes=N_NODES, max_sims=N_SIMS, time_steps=T_MS, bold_tr=TR, window_size=WS, window_step=STEP,
+                   bold_remove_s=REMOVE_S, noise_seed=410, device=local)
+    plan = B.Plan(cfg, sc, emp_fc, emp_fcd)
+    outputs = ("w_ie",)  # the reference returns corr, fic_penalties, w_IE_fic, FIC_failed, fic_n_trials
+    for _ in range(args.warmup):
+        plan.run(G, wEE, wEI, outputs=outputs)
+
+    def barrier():
+        if dist:
+            import torch
+            torch.cuda.synchronize()
+            dist.barrier()
+
+    barrier()
+    dev_ms, integ_ms, wall, flops = [], [], [], []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            r = plan.run(G, wEE, wEI, outputs=outputs)
+            if dist:
+                import torch
+                c = torch.tensor(r["cost"], device=f"cuda:{local}")
+                gathered = [torch.empty_like(c) for _ in range(world)]
+                dist.all_gather(gathered, c)
+                torch.cuda.synchronize()
+            wall.append(time.perf_counter() - t0)
+            t = plan.timings()
+            dev_ms.append(t["total"])
+            integ_ms.append(t["integrate"])
+            subs = 10 * (T_MS + 1) + 100_000 * r["fic_ntrials"].astype(np.float64)
+            flops.append(2.0 * N_NODES * N_NODES * subs.sum())
+    barrier()
+    dev_total, wall_total = float(np.sum(dev_ms)) / 1e3, float(np.sum(wall))
+    if dist:
+        import torch
+        t = torch.tensor([dev_total, wall_total], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        dev_total, wall_total = t.tolist()
+    value = world * N_SIMS * args.steps / dev_total
+    e2e = world * N_SIMS * args.steps / wall_total
+    result = None
+    if rank == 0:
+        peak = B.measure_fp32_peak(local)
+        achieved = float(np.mean(np.array(flops) / (np.array(integ_ms) * 1e-3))) / 1e12
+        cpu = cpu_reference_sample(len(os.sched_getaffinity(0))) if (world == 1 and not args.no_cpu) else None
+        n, N = N_SIMS, N_NODES
+        result = {
+            "metric": "sims/s", "value": value, "unit": "sims/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dev_total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "nodes": N, "particles_per_gpu": n, "model_time_ms": T_MS,
+                       "tr_ms": TR, "window": WS, "step": STEP, "precision": "f32 integration, f64 FIC/centring",
+                       "noise": "philox table", "l2": "inputs larger than L2 (3.6 GB noise table, 1.4 GB window FC)",
+                       "parallelism": f"particles sharded over {world} GPU(s)"},
+            "e2e": {"value": e2e, "unit": "sims/s", "h2d_bytes_per_step": 8 * (n + 2 * n * N),
+                    "d2h_bytes_per_step": 8 * n * 5 + 4 * n * 3 + 8 * n * N},
+            "gpu_launches": args.steps * 5,
+            "roofline": {"bound": "fp32", "kernel": "integrate_fast_kernel", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
+                         "peak_source": "measured on this GPU by bnm_measure_fp32_peak (packed FP32 FMA chains)",
+                         "work": "2*N^2 FLOP per substep per particle (coupling FMAs only), FIC restarts included"},
+            "stage_ms": {k: float(v) for k, v in plan.timings().items()},
+            "clocks": clk.summary(),
+        }
+        if cpu is not None:
+            result["cpu_baseline"] = {"value": cpu[0], "unit": "sims/s", "cores": len(os.sched_getaffinity(0)),
+                                      "kind": "reference", "sample": cpu[1]["sample"]}
+    plan.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if result is not None:
+        print(json.dumps(result))
+    return 0
+
+
+def main():
+    global N_SIMS, T_MS, WORKLOAD
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
+    ap.add_argument("--particles", type=int, default=N_SIMS, help="profiling knob: particles per GPU")
+    ap.add_argument("--model-ms", type=int, default=T_MS, help="profiling knob: model time per simulation")
+    args = ap.parse_args()
+    if args.particles != N_SIMS or args.model_ms != T_MS:
+        N_SIMS, T_MS = args.particles, args.model_ms
+        WORKLOAD = f"profiling-case-N100-{T_MS // 1000}s-x{N_SIMS}"
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

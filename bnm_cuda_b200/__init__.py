@@ -84,6 +84,7 @@ def lib():
         L.bnm_analytic_fic.argtypes = [vp, i32, vp, vp, vp, vp, vp]
         L.bnm_last_timings.argtypes = [vp, vp]
         L.bnm_plan_noise.argtypes = [vp, C.c_int64, C.c_int64, vp]
+        L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
         L.bnm_run_simulations.argtypes = [vp] * 8 + [i32] * 6 + [vp, i32, vp, i32, i32, i32, i32, vp, i32, i32, i32,
                                                                  vp, vp, vp, vp]
         L.bnm_cmaes_params_default.argtypes = [C.POINTER(_CmaesParams)]
@@ -234,6 +235,13 @@ class Plan:
         out = np.zeros(n, np.float32)
         _check(lib().bnm_plan_noise(self._h, offset, n, _ptr(out)))
         return out
+
+
+def measure_fp32_peak(device: int = 0) -> float:
+    """FP32 FMA-pipe throughput of the device in TFLOP/s (packed FMA probe)."""
+    t = C.c_double()
+    _check(lib().bnm_measure_fp32_peak(device, C.byref(t)))
+    return t.value
 
 
 def run_simulations(G_list, w_EE_list, w_EI_list, w_IE_list, SC, *, time_steps, BOLD_TR, window_size, window_step,

@@ -31,6 +31,7 @@ CU = {
     "analysis.cu": [],
     "fic_noise.cu": [],
     "capi.cu": [],
+    "probe.cu": [],
 }
 CPP = ["cmaes.cpp"]
 HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h"]

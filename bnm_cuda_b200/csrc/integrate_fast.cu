@@ -2,19 +2,28 @@
 //
 // Same model and time loop as the reference's bnm kernel (bnm.cu:72-315) and
 // CPU path (bnm.cpp:167-290), re-laid out for Blackwell:
-//   * one thread per node, one CTA per particle (persistent over particles,
-//     two CTAs per SM); the CTA's SC block is staged once into shared memory
-//     with a TMA bulk copy (cp.async.bulk + mbarrier, no multicast), then each
-//     thread keeps its SC row in registers for the whole run, so the coupling
-//     sum G*J*(SC.S_E) reads only the broadcast S_E vector from shared memory;
-//   * the coupling row-dot uses packed FP32 FMA (fma.rn.f32x2, __ffma2_rn)
-//     over column pairs with four independent accumulators;
-//   * S_E is double buffered in shared memory so a substep needs one barrier;
-//   * the next millisecond's noise (10 substeps x (E, I)) is prefetched into
-//     registers while the current one is integrated;
+//   * one CTA per particle (persistent over particles, two CTAs per SM); warp
+//     w owns nodes 32w..32w+31.  The coupling G*J*(SC.S_E) is a register-
+//     blocked mat-vec: lane l = 4u+v of warp w keeps the 4 x K block
+//     SC[32w+4u .. 32w+4u+3][Kv .. Kv+K-1] in registers for the whole run,
+//     reads only its K entries of S_E (broadcast LDS.128), and the four lanes
+//     of a row group finish with a 3-shuffle reduce-scatter after which lane l
+//     holds the full sum of node 32w+l.  Shared-memory traffic per substep is
+//     K floats per lane instead of N;
+//   * SC is staged once into shared memory by a TMA bulk copy (cp.async.bulk
+//     + mbarrier, no multicast, bounded wait) before being read into registers;
+//   * the row dot products use packed FP32 FMA (fma.rn.f32x2) over column
+//     pairs, two accumulators per row;
+//   * S_E is double buffered in shared memory: one barrier per substep;
+//   * the next millisecond's noise is prefetched into registers;
 //   * firing rates use ex2.approx / rcp.approx with an exact-limit series for
 //     |d(aI-b)| < 0.1, where 1-exp(-u) cancels (the reference FP32 build
 //     clamps |aI-b| to 1e-4 instead, bnm.cu:195-199);
+//   * the Balloon-Windkessel state is integrated as deviations from rest
+//     (f-1, nu-1, q-1, with log1p / expm1), so FP32 keeps full relative
+//     precision in the small BOLD fluctuations; the update order is the
+//     reference's (x, then f from the new x, nu from the old f, q from the old
+//     f and the new nu, bnm.cpp:204-211);
 //   * FIC sampling and the extended-output sums accumulate in FP64.
 #include "kernels.h"
 #define BNM_GENERIC_NS fastgen
@@ -25,11 +34,6 @@ namespace bnm {
 __device__ __forceinline__ float ex2_approx(float x) {
     float y;
     asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float lg2_approx(float x) {
-    float y;
-    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 __device__ __forceinline__ float rcp_approx(float x) {
@@ -71,24 +75,57 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
     return false;
 }
 
-template <int KMAX>
+// Balloon-Windkessel in deviation variables ft = f-1, nt = nu-1, qt = q-1.
+struct BW {
+    float x = 0.f, ft = 0.f, nt = 0.f, qt = 0.f;
+    __device__ __forceinline__ void step(float S_E) {
+        typedef Model<float> C;
+        const float L1mr = -0.41551544396166582f;  // ln(1 - rho)
+        const float a1 = C::ialpha - 1.0f;         // exponent of nu in nu^(1/alpha) q / nu
+        x = x + C::model_dt * (S_E - C::kappa * x - C::y * ft);
+        const float ft_new = ft + C::model_dt * x;
+        const float pw = expm1f(C::ialpha * log1pf(nt));  // nu^(1/alpha) - 1, old nu
+        const float f_old = 1.0f + ft;
+        const float nt_new = nt + C::model_dt * C::itau * (ft - pw);
+        // f (1 - (1-rho)^(1/f)) / rho - 1, without cancellation:
+        // 1 - (1-rho)^(1/f) - rho = -(1-rho) expm1(ln(1-rho) (1/f - 1))
+        const float h = -(1.0f - C::rho) * expm1f(-L1mr * ft / f_old);
+        const float inflow = (h + ft * (C::rho + h)) * (1.0f / C::rho);
+        // nu^(1/alpha - 1) q - 1 with the updated nu
+        const float e = expm1f(a1 * log1pf(nt_new));
+        const float outflow = e + qt * (1.0f + e);
+        qt = qt + C::model_dt * C::itau * (inflow - outflow);
+        nt = nt_new;
+        ft = ft_new;
+    }
+    __device__ __forceinline__ float bold() const {
+        typedef Model<float> C;
+        // V0 (k1 (1-q) + k2 (1 - q/nu) + k3 (1-nu))
+        return C::V_0 * (-C::k1 * qt + C::k2 * (nt - qt) / (1.0f + nt) - C::k3 * nt);
+    }
+};
+
+template <int K>
 __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
-    static_assert(KMAX % 8 == 0 && KMAX <= 128, "KMAX");
+    static_assert(K % 4 == 0 && K <= 32, "K");
+    constexpr int LD = 4 * K;  // padded SC row length and S_E buffer length
     typedef Model<float> C;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // layout: [SC stage: N*KMAX floats][S: 2*KMAX floats][mbarrier]
+    // layout: [SC stage: N*LD floats][S: 2*LD floats][mbarrier]
     const int N = a.N;
     float* sc_stage = reinterpret_cast<float*>(smem_raw);
-    float* S_buf = sc_stage + (size_t)N * KMAX;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(S_buf + 2 * KMAX);
+    float* S_buf = sc_stage + (size_t)N * LD;
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(S_buf + 2 * LD);
     __shared__ int s_sim;
 
-    const int j = threadIdx.x;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int u = lane >> 2, v = lane & 3;
+    const int j = threadIdx.x;  // node owned after the reduce-scatter (32w + lane)
     const bool act = j < N;
 
     // ---- stage SC into shared memory with one TMA bulk copy --------------
     const uint32_t bar = smem_addr(mbar);
-    const uint32_t bytes = (uint32_t)(N * KMAX * sizeof(float));
+    const uint32_t bytes = (uint32_t)(N * LD * sizeof(float));
     if (threadIdx.x == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -104,14 +141,18 @@ __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
     }
     if (!mbar_wait(bar, 0, 1ll << 26)) {
         if (threadIdx.x == 0) atomicOr(a.status, kStatusTimeout);
-        // the copy may still land in shared memory; wait (bounded) before exiting
-        mbar_wait(bar, 0, 1ll << 26);
+        mbar_wait(bar, 0, 1ll << 26);  // let a late copy land before the CTA exits
         return;
     }
-    float2 sc[KMAX / 2];
+    // this lane's 4 x K block of SC, as column pairs
+    float2 sc[4][K / 2];
 #pragma unroll
-    for (int m = 0; m < KMAX / 2; m++) {
-        sc[m] = act ? reinterpret_cast<const float2*>(sc_stage + (size_t)j * KMAX)[m] : make_float2(0.f, 0.f);
+    for (int r = 0; r < 4; r++) {
+        const int row = 32 * w + 4 * u + r;
+#pragma unroll
+        for (int c = 0; c < K / 2; c++)
+            sc[r][c] = row < N ? reinterpret_cast<const float2*>(sc_stage + (size_t)row * LD + v * K)[c]
+                               : make_float2(0.f, 0.f);
     }
 
     const float2* noise2 = reinterpret_cast<const float2*>(a.noise);
@@ -119,7 +160,6 @@ __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
     const double duration = (double)(a.samp_end - a.samp_start + 1);
     const float SQ = C::sigma_model * C::sqrt_dt;
     const float LOG2E = 1.4426950408889634f;
-    const float log2_1mrho = -0.59946207279f;  // log2(1 - 0.34)
 
     for (;;) {
         __syncthreads();
@@ -133,11 +173,12 @@ __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
         const float wEI = act ? (float)a.wEI[(size_t)sim * N + j] : 0.f;
         float wIE = act ? (float)a.wIE[(size_t)sim * N + j] : 0.f;
         float delta = (float)a.init_delta;
-        float S_E = 0.001f, S_I = 0.001f, x = 0.f, f = 1.f, nu = 1.f, q = 1.f;
+        float S_E = 0.001f, S_I = 0.001f;
+        BW bw;
         float IE = 0.f, II = 0.f, rE = 0.f, rI = 0.f;
         double mean_IE = 0.0;
         double ext[6] = {0, 0, 0, 0, 0, 0};
-        for (int k = threadIdx.x; k < 2 * KMAX; k += blockDim.x) S_buf[k] = (k < N) ? S_E : 0.f;
+        for (int k = threadIdx.x; k < 2 * LD; k += blockDim.x) S_buf[k] = ((k % LD) < N) ? S_E : 0.f;
         int cur = 0, trial = 0, ts = 0, frame = 0;
         bool failed = false, adjusting = a.adjust_fic != 0;
 
@@ -147,25 +188,39 @@ __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
         __syncthreads();
 
         while (ts <= a.T) {
-            // prefetch the next millisecond's noise
-            if (act && ts < a.T) {
+            if (act && ts < a.T) {  // prefetch the next millisecond's noise
                 const float2* src = noise2 + ((size_t)(ts + 1) * 10) * sub_stride + j;
 #pragma unroll
                 for (int s = 0; s < 10; s++) nz_next[s] = __ldg(src + (size_t)s * sub_stride);
             }
 #pragma unroll
             for (int sub = 0; sub < 10; sub++) {
-                const float4* S4 = reinterpret_cast<const float4*>(S_buf + cur * KMAX);
-                float2 acc0 = make_float2(0.f, 0.f), acc1 = acc0, acc2 = acc0, acc3 = acc0;
+                const float4* S4 = reinterpret_cast<const float4*>(S_buf + cur * LD + v * K);
+                float2 acc[4][2];
 #pragma unroll
-                for (int qd = 0; qd < KMAX / 8; qd++) {
-                    const float4 s0 = S4[2 * qd], s1 = S4[2 * qd + 1];
-                    acc0 = __ffma2_rn(sc[4 * qd + 0], make_float2(s0.x, s0.y), acc0);
-                    acc1 = __ffma2_rn(sc[4 * qd + 1], make_float2(s0.z, s0.w), acc1);
-                    acc2 = __ffma2_rn(sc[4 * qd + 2], make_float2(s1.x, s1.y), acc2);
-                    acc3 = __ffma2_rn(sc[4 * qd + 3], make_float2(s1.z, s1.w), acc3);
+                for (int r = 0; r < 4; r++) acc[r][0] = acc[r][1] = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int c4 = 0; c4 < K / 4; c4++) {
+                    const float4 s = S4[c4];
+                    const float2 s01 = make_float2(s.x, s.y), s23 = make_float2(s.z, s.w);
+#pragma unroll
+                    for (int r = 0; r < 4; r++) {
+                        acc[r][0] = __ffma2_rn(sc[r][2 * c4], s01, acc[r][0]);
+                        acc[r][1] = __ffma2_rn(sc[r][2 * c4 + 1], s23, acc[r][1]);
+                    }
                 }
-                const float coupling = ((acc0.x + acc0.y) + (acc1.x + acc1.y)) + ((acc2.x + acc2.y) + (acc3.x + acc3.y));
+                float p[4];
+#pragma unroll
+                for (int r = 0; r < 4; r++) p[r] = (acc[r][0].x + acc[r][0].y) + (acc[r][1].x + acc[r][1].y);
+                // reduce-scatter over the 4 lanes of this row group: lane v gets row 4u+v
+                const bool hi = (v >> 1) & 1, lo = v & 1;
+                const float k0 = hi ? p[2] : p[0], k1 = hi ? p[3] : p[1];
+                const float s0 = hi ? p[0] : p[2], s1 = hi ? p[1] : p[3];
+                const float q0 = k0 + __shfl_xor_sync(0xffffffffu, s0, 2);
+                const float q1 = k1 + __shfl_xor_sync(0xffffffffu, s1, 2);
+                const float kk = lo ? q1 : q0, ss = lo ? q0 : q1;
+                const float coupling = kk + __shfl_xor_sync(0xffffffffu, ss, 1);
+
                 IE = fmaf(GJ, coupling, fmaf(wEE, S_E, C::w_E__I_0)) - wIE * S_I;
                 II = fmaf(wEI, S_E, C::w_I__I_0) - S_I;
                 rE = rate(fmaf(C::a_E, IE, -C::b_E), C::d_E, 1.0f / C::d_E, -C::d_E * LOG2E);
@@ -175,23 +230,14 @@ __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
                 const float dSI = fmaf(n.y, SQ, C::dt * fmaf(C::gamma_I, rI, -S_I * (1.f / C::tau_I)));
                 S_E = fminf(fmaxf(S_E + dSE, 0.f), 1.f);
                 S_I = fminf(fmaxf(S_I + dSI, 0.f), 1.f);
-                if (act) S_buf[(cur ^ 1) * KMAX + j] = S_E;
+                if (act) S_buf[(cur ^ 1) * LD + j] = S_E;
                 __syncthreads();
                 cur ^= 1;
             }
-            // Balloon-Windkessel once per ms (nu is updated before q uses it,
-            // as in bnm.cpp:208-209)
-            x = x + C::model_dt * (S_E - C::kappa * x - C::y * (f - 1.f));
-            const float tmp_f = f + C::model_dt * x;
-            nu = nu + C::model_dt * C::itau * (f - ex2_approx(C::ialpha * lg2_approx(nu)));
-            const float inv_nu = rcp_approx(nu);
-            const float flow = f * (1.f - ex2_approx(log2_1mrho * rcp_approx(f))) * (1.f / C::rho);
-            q = q + C::model_dt * C::itau * (flow - ex2_approx(C::ialpha * lg2_approx(nu)) * q * inv_nu);
-            f = tmp_f;
+            bw.step(S_E);
             if (ts % a.TR == 0) {
                 if (act) {
-                    const float b = C::V_0 * (C::k1 * (1.f - q) + C::k2 * (1.f - q * inv_nu) + C::k3 * (1.f - nu));
-                    a.bold[((size_t)sim * a.frames + frame) * N + j] = b;
+                    a.bold[((size_t)sim * a.frames + frame) * N + j] = bw.bold();
                     if (frame >= a.n_vols_remove) {
                         ext[0] += S_E;
                         ext[1] += IE;
@@ -226,14 +272,11 @@ __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
                         if (trial < a.max_trials) {
                             S_E = 0.001f;
                             S_I = 0.001f;
-                            x = 0.f;
-                            f = 1.f;
-                            nu = 1.f;
-                            q = 1.f;
+                            bw = BW();
                             mean_IE = 0.0;
 #pragma unroll
-                            for (int v = 0; v < 6; v++) ext[v] = 0.0;
-                            if (act) S_buf[cur * KMAX + j] = S_E;
+                            for (int q = 0; q < 6; q++) ext[q] = 0.0;
+                            if (act) S_buf[cur * LD + j] = S_E;
                             ts = 0;
                             frame = 0;
                             trial++;
@@ -257,7 +300,7 @@ __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
             a.wIE_out[(size_t)sim * N + j] = (double)wIE;
             const double kept = (double)(frame - a.n_vols_remove);
 #pragma unroll
-            for (int v = 0; v < 6; v++) a.ext[((size_t)sim * 6 + v) * N + j] = ext[v] / kept;
+            for (int q = 0; q < 6; q++) a.ext[((size_t)sim * 6 + q) * N + j] = ext[q] / kept;
         }
         if (threadIdx.x == 0) {
             a.trials[sim] = trial;
@@ -266,39 +309,39 @@ __global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
     }
 }
 
-
-template <int KMAX>
+template <int K>
 static cudaError_t launch_fast(const SimArgs& a, int grid, cudaStream_t st) {
     const int threads = ((a.N + 31) / 32) * 32;
-    const size_t smem = (size_t)a.N * KMAX * sizeof(float) + 2 * KMAX * sizeof(float) + 16;
-    cudaError_t e = cudaFuncSetAttribute(integrate_fast_kernel<KMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    const size_t smem = (size_t)a.N * 4 * K * sizeof(float) + 2 * 4 * K * sizeof(float) + 16;
+    cudaError_t e =
+        cudaFuncSetAttribute(integrate_fast_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    integrate_fast_kernel<KMAX><<<grid, threads, smem, st>>>(a);
+    integrate_fast_kernel<K><<<grid, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 
 }  // namespace bnm
 
-// Padded row length of the register-resident SC for a node count (0 = the
-// fast kernel does not cover it).
+// Padded SC row length (4K) of the register kernel for a node count (0 = the
+// register kernel does not cover it).
 extern "C" int bnm_fast_kmax(int N) {
     if (N <= 0 || N > 128) return 0;
-    return ((N + 7) / 8) * 8;
+    const int K = ((N + 3) / 4 + 3) / 4 * 4;
+    return 4 * K;
 }
 
 // FP32 launch: the register-SC kernel when N <= 128, else the reference-order
 // kernel in float (SC from shared memory when it fits, else from L2).
 cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStream_t st) {
     using namespace bnm;
-    const int kmax = bnm_fast_kmax(a.N);
-    if (kmax) {
+    const int ld = bnm_fast_kmax(a.N);
+    if (ld) {
+        if (a.sc_ld != ld) return cudaErrorInvalidValue;
         const int grid = a.n_sims < 2 * num_sms ? a.n_sims : 2 * num_sms;
-        switch (kmax) {
+        switch (ld / 4) {
 #define BNM_K(K) \
     case K: return launch_fast<K>(a, grid, st);
-            BNM_K(8) BNM_K(16) BNM_K(24) BNM_K(32) BNM_K(40) BNM_K(48) BNM_K(56) BNM_K(64) BNM_K(72) BNM_K(80)
-            BNM_K(88) BNM_K(96) BNM_K(104) BNM_K(112) BNM_K(120) BNM_K(128)
+            BNM_K(4) BNM_K(8) BNM_K(12) BNM_K(16) BNM_K(20) BNM_K(24) BNM_K(28) BNM_K(32)
 #undef BNM_K
             default: return cudaErrorInvalidValue;
         }
@@ -309,8 +352,8 @@ cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStr
     const size_t sc_bytes = (size_t)a.N * a.sc_ld * sizeof(float);
     int sc_in_smem = (smem + sc_bytes) <= 200 * 1024;
     if (sc_in_smem) smem += sc_bytes;
-    cudaError_t e = cudaFuncSetAttribute(fastgen::integrate_generic_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(fastgen::integrate_generic_kernel<float>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = a.n_sims < 2 * num_sms ? a.n_sims : 2 * num_sms;
     fastgen::integrate_generic_kernel<float><<<grid, threads, smem, st>>>(a, sc_in_smem);

@@ -1,0 +1,55 @@
+// FP32 FMA-pipe throughput probe.  The measured peak tables in the repo hold
+// HBM copy bandwidth and tensor-core GEMM rates only; the integrator is bound
+// by the FP32 pipe, so its roofline denominator is measured here: eight
+// independent chains of packed FP32 FMA (fma.rn.f32x2) per thread, enough
+// CTAs for every SM, timed with CUDA events.
+#include <cuda_runtime.h>
+#include "../../include/bnm_b200.h"
+#include "kernels.h"
+
+int bnm_fail_cuda(cudaError_t e, const char* expr, const char* file, int line);
+
+__global__ void __launch_bounds__(256) ffma2_probe_kernel(float* out, int iters) {
+    float2 a[8];
+#pragma unroll
+    for (int i = 0; i < 8; i++) a[i] = make_float2(1.0f + 1e-3f * threadIdx.x + i, 0.5f + 1e-3f * i);
+    const float2 m = make_float2(0.99999f, 1.00001f), c = make_float2(1e-6f, -1e-6f);
+    for (int it = 0; it < iters; it++) {
+#pragma unroll
+        for (int i = 0; i < 8; i++) a[i] = __ffma2_rn(a[i], m, c);
+    }
+    float s = 0.f;
+#pragma unroll
+    for (int i = 0; i < 8; i++) s += a[i].x + a[i].y;
+    out[blockIdx.x * blockDim.x + threadIdx.x] = s;
+}
+
+extern "C" int bnm_measure_fp32_peak(int32_t device, double* tflops) {
+    BNM_CUDA_TRY(cudaSetDevice(device));
+    int sms = 0;
+    BNM_CUDA_TRY(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+    const int grid = sms * 8, block = 256, iters = 1 << 15;
+    float* out = nullptr;
+    BNM_CUDA_TRY(cudaMalloc(&out, (size_t)grid * block * sizeof(float)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0);
+        ffma2_probe_kernel<<<grid, block>>>(out, iters);
+        cudaEventRecord(e1);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (rep > 0 && ms < best) best = ms;
+    }
+    cudaError_t err = cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(out);
+    BNM_CUDA_TRY(err);
+    const double flops = (double)grid * block * iters * 8 * 2 * 2;
+    *tflops = flops / (best * 1e-3) / 1e12;
+    return BNM_OK;
+}

@@ -141,6 +141,11 @@ int bnm_analytic_fic(bnm_plan *plan, int32_t n, const double *G, const double *w
  * [0] analytic FIC, [1] integration, [2] FC + window FC, [3] FCD + KS histogram, [4] GOF, [5] total. */
 int bnm_last_timings(bnm_plan *plan, double *ms6);
 
+/* Measured FP32 FMA throughput of a device (packed fma.rn.f32x2 chains), in
+ * TFLOP/s: the roofline denominator of the FP32-pipe-bound integrator.  No
+ * counterpart in the reference. */
+int bnm_measure_fp32_peak(int32_t device, double *tflops);
+
 /* Device noise table of the plan, copied out (n floats from offset). */
 int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);
 
