@@ -1,0 +1,60 @@
+"""The drop-in CLI (bnm_cuda_b200/run_CMAES_gpu) on a small synthetic case:
+same arguments as the reference's run_CMAES (run_CMAES.cpp:192-218), same
+output directories, log lines and best-simulation files (bnm.cu:771-833)."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+ROOT = os.path.abspath(os.path.join(os.path.dirname(__file__), ".."))
+CLI = os.path.join(ROOT, "bnm_cuda_b200", "run_CMAES_gpu")
+
+
+def test_cli_usage_without_gpu():
+    out = subprocess.run([CLI], capture_output=True, text=True)
+    assert out.returncode == 0 and out.stdout.startswith("Usage: ./run_CMAES_")
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("het", ["none", "wee-wei"])
+def test_cli_runs_cmaes_and_writes_reference_files(tmp_path, golden, het):
+    g = golden["n10_t12s"]
+    N, T, TR, ws, step, remove, exc, nvr, seed = [int(v) for v in g["meta"]]
+    d = tmp_path / "sub-01"
+    d.mkdir()
+    np.savetxt(d / "SC.txt", g["sc"])
+    np.savetxt(d / "sub-01_desc-FCtril.txt", g["emp_fc"])
+    np.savetxt(d / "sub-01_desc-FCDtril.txt", g["emp_fcd"])
+    np.savetxt(d / "maps.txt", np.random.default_rng(0).standard_normal((2, N)))
+    lam, it_max = 6, 3
+    args = [CLI, str(d / "SC.txt"), "same", str(d / "sub-01_desc-FCtril.txt"), str(d / "sub-01_desc-FCDtril.txt"),
+            str(d / "maps.txt"), str(N), "0.5-3.5", "0.05-0.5", "0.05-0.5", "0", het, str(T), str(TR), str(step),
+            str(ws), "410", str(lam), str(it_max), "1"]
+    env = dict(os.environ, BNM_BOLD_REMOVE=str(remove))
+    r = subprocess.run(args, capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stderr + r.stdout
+    multi = "_multimaps" if het != "none" else ""
+    cm, sims = d / "SC" / f"cmaes{multi}_gpu", d / "SC" / f"sims{multi}_gpu"
+    logs = list(cm.iterdir())
+    assert len(logs) == 1
+    name = logs[0].name
+    assert name.startswith("sub-01_G_0.5-3.5_wee_0.05-0.5_wei_0.05-0.5_wie_0_het-" + het)
+    assert name.endswith(f"_SeedMW-1_SeedSim-410_n-{it_max}x{lam}.txt")
+    log = logs[0].read_text()
+    dim = 3 + (2 * 2 if het != "none" else 0)
+    assert log.startswith(f"Running {dim}D CMAES\nSC: ")
+    assert "Free parameters: G (0.500000-3.500000) " in log
+    assert len(re.findall(r"^Iteration \d+$", log, re.M)) == it_max - 1
+    rows = re.findall(r"^\t IndPar \d+: .*gof=(-?[\d.]+),fic_penalty=([\d.]+),penalized_cost=([\d.]+)$", log, re.M)
+    assert len(rows) == lam * (it_max - 1)
+    assert re.search(r"^Best feasible parameters: G=.*gof=-?[\d.]+,fic_penalty=[\d.]+,gof_fic_penalty=-?[\d.]+$",
+                     log, re.M)
+    prefix = name[:-4] + "_"
+    bold = np.loadtxt(sims / (prefix + "bold.txt"))
+    assert bold.shape == (T // TR + 1, N)
+    for f in ["S_E", "I_E", "r_E", "S_I", "I_I", "r_I", "w_EE", "w_EI", "w_IE"]:
+        assert np.loadtxt(sims / (prefix + f + ".txt")).shape == (N,)
+    assert (sims / (prefix + "fic_ntrials.txt")).read_text().endswith("of max 10")
+    assert (sims / (prefix + "fic_failed.txt")).read_text() in ("0", "1")
