@@ -85,6 +85,7 @@ def lib():
         L.bnm_last_timings.argtypes = [vp, vp]
         L.bnm_plan_noise.argtypes = [vp, C.c_int64, C.c_int64, vp]
         L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
+        L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
         L.bnm_run_simulations.argtypes = [vp] * 8 + [i32] * 6 + [vp, i32, vp, i32, i32, i32, i32, vp, i32, i32, i32,
                                                                  vp, vp, vp, vp]
         L.bnm_cmaes_params_default.argtypes = [C.POINTER(_CmaesParams)]
@@ -242,6 +243,21 @@ def measure_fp32_peak(device: int = 0) -> float:
     t = C.c_double()
     _check(lib().bnm_measure_fp32_peak(device, C.byref(t)))
     return t.value
+
+
+def gof_noalloc(d_bold: int, n: int, frames: int, nodes: int, n_vols_remove: int, window_size: int,
+                window_step: int, emp_fc, emp_fcd, d_out: int, *, exc_interhem=True, use_fc_diff=True,
+                max_cost=2.0, stream: int = 0) -> None:
+    """bnm_gof_noalloc: goodness of fit of ``n`` BOLD series already on the
+    device (``d_bold``: device address of float [n][frames][nodes]) into
+    ``d_out`` (device address of double [5][n]: cost, fc_corr, fc_diff,
+    fcd_ks, 0), using only the library's static device scratch array.
+    Asynchronous on ``stream``."""
+    efc = _d(emp_fc)
+    efcd = np.sort(_d(emp_fcd))
+    _check(lib().bnm_gof_noalloc(C.c_void_p(d_bold), n, frames, nodes, n_vols_remove, window_size, window_step,
+                                 int(exc_interhem), int(use_fc_diff), float(max_cost), _ptr(efc), len(efc),
+                                 _ptr(efcd), len(efcd), C.c_void_p(d_out), C.c_void_p(stream)))
 
 
 def run_simulations(G_list, w_EE_list, w_EI_list, w_IE_list, SC, *, time_steps, BOLD_TR, window_size, window_step,

@@ -32,6 +32,7 @@ CU = {
     "fic_noise.cu": [],
     "capi.cu": [],
     "probe.cu": [],
+    "noalloc.cu": [],
 }
 CPP = ["cmaes.cpp"]
 HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h"]

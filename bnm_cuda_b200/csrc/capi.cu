@@ -36,6 +36,8 @@ int bnm_fail_cuda(cudaError_t e, const char* expr, const char* file, int line) {
                 cudaGetErrorString(e), file, line);
 }
 
+int bnm_fail_msg(int code, const char* msg) { return fail(code, "%s", msg); }
+
 extern "C" const char* bnm_last_error(void) { return g_err.c_str(); }
 
 extern "C" int bnm_device_count(void) {

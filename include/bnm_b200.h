@@ -149,6 +149,31 @@ int bnm_measure_fp32_peak(int32_t device, double *tflops);
 /* Device noise table of the plan, copied out (n floats from offset). */
 int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);
 
+/* ------------------------------------------------ allocation-free entry
+ * No counterpart in the reference.  Goodness of fit (FC, sliding-window FC,
+ * FCD, KS, cost) of n BOLD series that are already on the device, for callers
+ * that cannot allocate device memory: hosts that own the allocator (an
+ * embedding framework's caching allocator or a fixed memory budget) and
+ * real-time or streaming loops that must not call cudaMalloc / cudaFree
+ * (cudaFree synchronises the device).  Nothing is allocated: every
+ * intermediate lives in one static device array of BNM_NOALLOC_SCRATCH_BYTES
+ * per device, resident on every GPU that loads the library until exit.
+ *   d_bold          device [n][frames][nodes] float
+ *   emp_fc          host [n_pairs], the reference's pair order
+ *   emp_fcd_sorted  host [n_emp_fcd], ascending (checked)
+ *   d_out           device [5][n] double: cost, fc_corr, fc_diff, fcd_ks, 0
+ *   stream          a cudaStream_t (NULL = the default stream); the call is
+ *                   asynchronous on it.
+ * Calls whose intermediates exceed the scratch array fail with BNM_EINVAL.
+ * All calls share the array: the call zeroes what it accumulates, but calls
+ * that overlap on the GPU race.  The first call on a device looks up the
+ * array's address; make it before any stream capture. */
+#define BNM_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
+int bnm_gof_noalloc(const float *d_bold, int32_t n, int32_t frames, int32_t nodes, int32_t n_vols_remove,
+                    int32_t window_size, int32_t window_step, int32_t exc_interhem, int32_t use_fc_diff,
+                    double max_cost, const double *emp_fc, int32_t n_emp_fc, const double *emp_fcd_sorted,
+                    int32_t n_emp_fcd, double *d_out, void *stream);
+
 /* ------------------------------------------------------ one-shot mirror
  * Same argument meaning as the reference's run_simulations (bnm.cu:594-617),
  * flattened: builds a plan, runs one batch, releases it.  corr receives the
