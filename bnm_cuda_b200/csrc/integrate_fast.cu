@@ -7,15 +7,20 @@
 //     blocked mat-vec: lane l = 4u+v of warp w keeps the 4 x K block
 //     SC[32w+4u .. 32w+4u+3][Kv .. Kv+K-1] in registers for the whole run,
 //     reads only its K entries of S_E (broadcast LDS.128), and the four lanes
-//     of a row group finish with a 3-shuffle reduce-scatter after which lane l
-//     holds the full sum of node 32w+l.  Shared-memory traffic per substep is
+//     of a row group finish with a select-free 3-shuffle reduce-scatter (rows
+//     stored in xor-permuted slots) after which lane l holds the full sum of
+//     node 32w+l.  Shared-memory traffic per substep is
 //     K floats per lane instead of N;
 //   * SC is staged once into shared memory by a TMA bulk copy (cp.async.bulk
 //     + mbarrier, no multicast, bounded wait) before being read into registers;
 //   * the row dot products use packed FP32 FMA (fma.rn.f32x2) over column
 //     pairs, two accumulators per row;
 //   * S_E is double buffered in shared memory: one barrier per substep;
-//   * the next millisecond's noise is prefetched into registers;
+//   * noise arrives one simulated millisecond at a time (10 substeps x N x
+//     (E, I), contiguous in the table) by TMA bulk copies into a 4-stage
+//     shared-memory ring, issued three milliseconds ahead by one thread and
+//     tracked with mbarriers; an FIC restart drains the copies in flight and
+//     refetches from millisecond 0;
 //   * firing rates use ex2.approx / rcp.approx with an exact-limit series for
 //     |d(aI-b)| < 0.1, where 1-exp(-u) cancels (the reference FP32 build
 //     clamps |aI-b| to 1e-4 instead, bnm.cu:195-199);
@@ -25,6 +30,7 @@
 //     reference's (x, then f from the new x, nu from the old f, q from the old
 //     f and the new nu, bnm.cpp:204-211);
 //   * FIC sampling and the extended-output sums accumulate in FP64.
+#include <cstdlib>
 #include "kernels.h"
 #define BNM_GENERIC_NS fastgen
 #include "integrate_generic.cuh"
@@ -77,25 +83,26 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
 
 // Balloon-Windkessel in deviation variables ft = f-1, nt = nu-1, qt = q-1.
 struct BW {
-    float x = 0.f, ft = 0.f, nt = 0.f, qt = 0.f;
+    float x = 0.f, ft = 0.f, nt = 0.f, qt = 0.f, lnu = 0.f;  // lnu = log(nu) = log1p(nt)
     __device__ __forceinline__ void step(float S_E) {
         typedef Model<float> C;
         const float L1mr = -0.41551544396166582f;  // ln(1 - rho)
         const float a1 = C::ialpha - 1.0f;         // exponent of nu in nu^(1/alpha) q / nu
         x = x + C::model_dt * (S_E - C::kappa * x - C::y * ft);
         const float ft_new = ft + C::model_dt * x;
-        const float pw = expm1f(C::ialpha * log1pf(nt));  // nu^(1/alpha) - 1, old nu
-        const float f_old = 1.0f + ft;
+        const float pw = expm1f(C::ialpha * lnu);  // nu^(1/alpha) - 1, old nu
         const float nt_new = nt + C::model_dt * C::itau * (ft - pw);
         // f (1 - (1-rho)^(1/f)) / rho - 1, without cancellation:
         // 1 - (1-rho)^(1/f) - rho = -(1-rho) expm1(ln(1-rho) (1/f - 1))
-        const float h = -(1.0f - C::rho) * expm1f(-L1mr * ft / f_old);
+        const float h = -(1.0f - C::rho) * expm1f(-L1mr * __fdividef(ft, 1.0f + ft));
         const float inflow = (h + ft * (C::rho + h)) * (1.0f / C::rho);
         // nu^(1/alpha - 1) q - 1 with the updated nu
-        const float e = expm1f(a1 * log1pf(nt_new));
+        const float lnu_new = log1pf(nt_new);
+        const float e = expm1f(a1 * lnu_new);
         const float outflow = e + qt * (1.0f + e);
         qt = qt + C::model_dt * C::itau * (inflow - outflow);
         nt = nt_new;
+        lnu = lnu_new;
         ft = ft_new;
     }
     __device__ __forceinline__ float bold() const {
@@ -105,218 +112,335 @@ struct BW {
     }
 };
 
-template <int K>
-__global__ void __launch_bounds__(128, 2) integrate_fast_kernel(SimArgs a) {
+// Noise ring: the 10 substeps x N nodes x (E, I) floats of one simulated
+// millisecond are contiguous in the table (80 N bytes), so one thread brings a
+// whole millisecond into shared memory with one TMA bulk copy.  kStages
+// copies are in flight ahead of the consumer; copy c lives in stage c % kStages
+// and completes phase (c / kStages) & 1 of that stage's mbarrier.
+constexpr int kStages = 4;
+
+// Per-particle ("slot") state that every thread keeps for its node.
+struct Slot {
+    float GJ, wEE, wEI, wIE, delta, S_E, S_I, IE, II, rE, rI;
+    double mean_IE;
+    BW bw;
+};
+
+// One CTA integrates P particles at a time (P slots) with the same warps:
+// the SC block in registers serves every slot, so the slots' independent
+// dependency chains interleave inside each warp (instruction-level
+// parallelism instead of a second CTA on the SM).  Slots advance one
+// simulated millisecond per iteration in lockstep but keep their own time,
+// FIC trial and noise stream; a slot whose particle ends takes the next one
+// from the batch's work counter.
+template <int K, int P>
+__global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     static_assert(K % 4 == 0 && K <= 32, "K");
+    static_assert(P >= 1 && P <= 2, "P");
     constexpr int LD = 4 * K;  // padded SC row length and S_E buffer length
     typedef Model<float> C;
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    // layout: [SC stage: N*LD floats][S: 2*LD floats][mbarrier]
+    // layout: [noise rings: P * kStages * 10*N float2][SC stage: N*LD floats]
+    //         [S: P * 2*LD floats][extended sums: P*6*blockDim doubles][mbarriers: 1 + P*kStages]
     const int N = a.N;
-    float* sc_stage = reinterpret_cast<float*>(smem_raw);
+    const uint32_t ms_bytes = (uint32_t)(10 * N * sizeof(float2));
+    float2* ring = reinterpret_cast<float2*>(smem_raw);
+    float* sc_stage = reinterpret_cast<float*>(smem_raw + (size_t)P * kStages * ms_bytes);
     float* S_buf = sc_stage + (size_t)N * LD;
-    uint64_t* mbar = reinterpret_cast<uint64_t*>(S_buf + 2 * LD);
-    __shared__ int s_sim;
+    double* ext = reinterpret_cast<double*>(S_buf + P * 2 * LD);
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(ext + (size_t)P * 6 * blockDim.x);
+    __shared__ int s_sim[P], s_flag;
 
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int u = lane >> 2, v = lane & 3;
     const int j = threadIdx.x;  // node owned after the reduce-scatter (32w + lane)
     const bool act = j < N;
+    const long long kSpin = 1ll << 26;
 
-    // ---- stage SC into shared memory with one TMA bulk copy --------------
-    const uint32_t bar = smem_addr(mbar);
-    const uint32_t bytes = (uint32_t)(N * LD * sizeof(float));
+    // ---- barriers; stage SC into shared memory with one TMA bulk copy ----
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        for (int b = 0; b <= P * kStages; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + b)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     __syncthreads();
+    const uint32_t sc_bytes = (uint32_t)(N * LD * sizeof(float));
     if (threadIdx.x == 0) {
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar)), "r"(sc_bytes)
+                     : "memory");
         asm volatile(
             "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
                 smem_addr(sc_stage)),
-            "l"(a.sc_f32), "r"(bytes), "r"(bar)
+            "l"(a.sc_f32), "r"(sc_bytes), "r"(smem_addr(mbar))
             : "memory");
     }
-    if (!mbar_wait(bar, 0, 1ll << 26)) {
+    if (__syncthreads_or(!mbar_wait(smem_addr(mbar), 0, kSpin))) {
         if (threadIdx.x == 0) atomicOr(a.status, kStatusTimeout);
-        mbar_wait(bar, 0, 1ll << 26);  // let a late copy land before the CTA exits
+        mbar_wait(smem_addr(mbar), 0, kSpin);  // let a late copy land before the CTA exits
         return;
     }
-    // this lane's 4 x K block of SC, as column pairs
+    // This lane's 4 x K block of SC as column pairs.  Slot r of a lane holds
+    // row 4u + (v ^ r), so the reduce-scatter below keeps slot 0 and needs no
+    // selects: after the xor-2 exchange slots 0 / 1 hold rows v / v^1, after
+    // the xor-1 exchange slot 0 holds the full sum of row 4u + v.
     float2 sc[4][K / 2];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
-        const int row = 32 * w + 4 * u + r;
+        const int row = 32 * w + 4 * u + (v ^ r);
 #pragma unroll
         for (int c = 0; c < K / 2; c++)
             sc[r][c] = row < N ? reinterpret_cast<const float2*>(sc_stage + (size_t)row * LD + v * K)[c]
                                : make_float2(0.f, 0.f);
     }
 
-    const float2* noise2 = reinterpret_cast<const float2*>(a.noise);
-    const size_t sub_stride = (size_t)N;  // float2 entries per substep
+    const char* noise_bytes = reinterpret_cast<const char*>(a.noise);
     const double duration = (double)(a.samp_end - a.samp_start + 1);
     const float SQ = C::sigma_model * C::sqrt_dt;
     const float LOG2E = 1.4426950408889634f;
+    const float kDtGammaE = C::dt * C::gamma_E, kDtInvTauE = C::dt / C::tau_E;
+    const float kDtGammaI = C::dt * C::gamma_I, kDtInvTauI = C::dt / C::tau_I;
+
+    // per-slot control (uniform over the CTA); thread 0 also owns the copy issue state
+    int sim[P], ts[P], frame[P], to_frame[P], trial[P], ms_next[P];
+    bool failed[P], adjusting[P], live[P];
+    uint32_t c_cons[P], c_issue[P];
+    Slot sl[P];
+    bool timed_out = false;
+
+    auto wait_copy = [&](int p, uint32_t c) -> bool {
+        return mbar_wait(smem_addr(mbar + 1 + p * kStages + c % kStages), (c / kStages) & 1, kSpin);
+    };
+    auto issue = [&](int p) {  // thread 0: keep up to kStages copies ahead of slot p's consumer
+        while (c_issue[p] < c_cons[p] + kStages && ms_next[p] <= a.T) {
+            const uint32_t st = c_issue[p] % kStages;
+            const uint32_t bar = smem_addr(mbar + 1 + p * kStages + st);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(ms_bytes)
+                         : "memory");
+            asm volatile(
+                "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                    smem_addr(ring + ((size_t)p * kStages + st) * 10 * N)),
+                "l"(noise_bytes + (size_t)ms_next[p] * ms_bytes), "r"(ms_bytes), "r"(bar)
+                : "memory");
+            c_issue[p]++;
+            ms_next[p]++;
+        }
+    };
+    // take the next particle of the batch into slot p (all threads)
+    auto load = [&](int p) {
+        if (threadIdx.x == 0) s_sim[p] = atomicAdd(a.work_counter, 1);
+        __syncthreads();
+        sim[p] = s_sim[p];
+        live[p] = sim[p] < a.n_sims;
+        const int sm = live[p] ? sim[p] : 0;
+        Slot& q = sl[p];
+        q.GJ = (float)a.G[sm] * C::J_NMDA;
+        q.wEE = act ? (float)a.wEE[(size_t)sm * N + j] : 0.f;
+        q.wEI = act ? (float)a.wEI[(size_t)sm * N + j] : 0.f;
+        q.wIE = act ? (float)a.wIE[(size_t)sm * N + j] : 0.f;
+        q.delta = (float)a.init_delta;
+        q.S_E = q.S_I = 0.001f;
+        q.IE = q.II = q.rE = q.rI = 0.f;
+        q.mean_IE = 0.0;
+        q.bw = BW();
+#pragma unroll
+        for (int e = 0; e < 6; e++) ext[((size_t)p * 6 + e) * blockDim.x + threadIdx.x] = 0.0;
+        for (int k = threadIdx.x; k < 2 * LD; k += blockDim.x) S_buf[p * 2 * LD + k] = ((k % LD) < N) ? 0.001f : 0.f;
+        ts[p] = 0;
+        frame[p] = 0;
+        to_frame[p] = 1;
+        trial[p] = 0;
+        failed[p] = false;
+        adjusting[p] = a.adjust_fic != 0;
+        ms_next[p] = 0;
+        __syncthreads();
+    };
+#pragma unroll
+    for (int p = 0; p < P; p++) {
+        c_cons[p] = c_issue[p] = 0;
+        load(p);
+    }
+    int cur = 0;
 
     for (;;) {
-        __syncthreads();
-        if (threadIdx.x == 0) s_sim = atomicAdd(a.work_counter, 1);
-        __syncthreads();
-        const int sim = s_sim;
-        if (sim >= a.n_sims) break;
+        bool any = false;
+#pragma unroll
+        for (int p = 0; p < P; p++) any |= live[p];
+        if (!any) break;
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int p = 0; p < P; p++)
+                if (live[p]) issue(p);
+        }
+        bool late = false;
+#pragma unroll
+        for (int p = 0; p < P; p++)
+            if (live[p]) late |= !wait_copy(p, c_cons[p]);
+        if (__syncthreads_or(late)) {
+            timed_out = true;
+            break;
+        }
+        const float2* nz[P];
+#pragma unroll
+        for (int p = 0; p < P; p++) nz[p] = ring + ((size_t)p * kStages + c_cons[p] % kStages) * 10 * N + j;
 
-        const float GJ = (float)a.G[sim] * C::J_NMDA;
-        const float wEE = act ? (float)a.wEE[(size_t)sim * N + j] : 0.f;
-        const float wEI = act ? (float)a.wEI[(size_t)sim * N + j] : 0.f;
-        float wIE = act ? (float)a.wIE[(size_t)sim * N + j] : 0.f;
-        float delta = (float)a.init_delta;
-        float S_E = 0.001f, S_I = 0.001f;
-        BW bw;
-        float IE = 0.f, II = 0.f, rE = 0.f, rI = 0.f;
-        double mean_IE = 0.0;
-        double ext[6] = {0, 0, 0, 0, 0, 0};
-        for (int k = threadIdx.x; k < 2 * LD; k += blockDim.x) S_buf[k] = ((k % LD) < N) ? S_E : 0.f;
-        int cur = 0, trial = 0, ts = 0, frame = 0;
-        bool failed = false, adjusting = a.adjust_fic != 0;
-
-        float2 nz[10], nz_next[10];
 #pragma unroll
-        for (int s = 0; s < 10; s++) nz[s] = act ? __ldg(noise2 + (size_t)s * sub_stride + j) : make_float2(0.f, 0.f);
-        __syncthreads();
-
-        while (ts <= a.T) {
-            if (act && ts < a.T) {  // prefetch the next millisecond's noise
-                const float2* src = noise2 + ((size_t)(ts + 1) * 10) * sub_stride + j;
+        for (int sub = 0; sub < 10; sub++) {
+            float2 acc[P][4];
 #pragma unroll
-                for (int s = 0; s < 10; s++) nz_next[s] = __ldg(src + (size_t)s * sub_stride);
-            }
+            for (int p = 0; p < P; p++)
 #pragma unroll
-            for (int sub = 0; sub < 10; sub++) {
-                const float4* S4 = reinterpret_cast<const float4*>(S_buf + cur * LD + v * K);
-                float2 acc[4][2];
+                for (int r = 0; r < 4; r++) acc[p][r] = make_float2(0.f, 0.f);
 #pragma unroll
-                for (int r = 0; r < 4; r++) acc[r][0] = acc[r][1] = make_float2(0.f, 0.f);
+            for (int c4 = 0; c4 < K / 4; c4++) {
 #pragma unroll
-                for (int c4 = 0; c4 < K / 4; c4++) {
-                    const float4 s = S4[c4];
+                for (int p = 0; p < P; p++) {
+                    const float4 s = reinterpret_cast<const float4*>(S_buf + (p * 2 + cur) * LD + v * K)[c4];
                     const float2 s01 = make_float2(s.x, s.y), s23 = make_float2(s.z, s.w);
 #pragma unroll
                     for (int r = 0; r < 4; r++) {
-                        acc[r][0] = __ffma2_rn(sc[r][2 * c4], s01, acc[r][0]);
-                        acc[r][1] = __ffma2_rn(sc[r][2 * c4 + 1], s23, acc[r][1]);
+                        acc[p][r] = __ffma2_rn(sc[r][2 * c4], s01, acc[p][r]);
+                        acc[p][r] = __ffma2_rn(sc[r][2 * c4 + 1], s23, acc[p][r]);
                     }
                 }
-                float p[4];
+            }
 #pragma unroll
-                for (int r = 0; r < 4; r++) p[r] = (acc[r][0].x + acc[r][0].y) + (acc[r][1].x + acc[r][1].y);
-                // reduce-scatter over the 4 lanes of this row group: lane v gets row 4u+v
-                const bool hi = (v >> 1) & 1, lo = v & 1;
-                const float k0 = hi ? p[2] : p[0], k1 = hi ? p[3] : p[1];
-                const float s0 = hi ? p[0] : p[2], s1 = hi ? p[1] : p[3];
-                const float q0 = k0 + __shfl_xor_sync(0xffffffffu, s0, 2);
-                const float q1 = k1 + __shfl_xor_sync(0xffffffffu, s1, 2);
-                const float kk = lo ? q1 : q0, ss = lo ? q0 : q1;
-                const float coupling = kk + __shfl_xor_sync(0xffffffffu, ss, 1);
-
-                IE = fmaf(GJ, coupling, fmaf(wEE, S_E, C::w_E__I_0)) - wIE * S_I;
-                II = fmaf(wEI, S_E, C::w_I__I_0) - S_I;
-                rE = rate(fmaf(C::a_E, IE, -C::b_E), C::d_E, 1.0f / C::d_E, -C::d_E * LOG2E);
-                rI = rate(fmaf(C::a_I, II, -C::b_I), C::d_I, 1.0f / C::d_I, -C::d_I * LOG2E);
-                const float2 n = nz[sub];
-                const float dSE = fmaf(n.x, SQ, C::dt * fmaf((1.f - S_E) * C::gamma_E, rE, -S_E * (1.f / C::tau_E)));
-                const float dSI = fmaf(n.y, SQ, C::dt * fmaf(C::gamma_I, rI, -S_I * (1.f / C::tau_I)));
-                S_E = fminf(fmaxf(S_E + dSE, 0.f), 1.f);
-                S_I = fminf(fmaxf(S_I + dSI, 0.f), 1.f);
-                if (act) S_buf[(cur ^ 1) * LD + j] = S_E;
-                __syncthreads();
-                cur ^= 1;
+            for (int p = 0; p < P; p++) {
+                Slot& q = sl[p];
+                // reduce-scatter over the 4 lanes of this row group (see the SC slot order)
+                const float q0 =
+                    (acc[p][0].x + acc[p][0].y) + __shfl_xor_sync(0xffffffffu, acc[p][2].x + acc[p][2].y, 2);
+                const float q1 =
+                    (acc[p][1].x + acc[p][1].y) + __shfl_xor_sync(0xffffffffu, acc[p][3].x + acc[p][3].y, 2);
+                const float coupling = q0 + __shfl_xor_sync(0xffffffffu, q1, 1);
+                const float2 n = act ? nz[p][(size_t)sub * N] : make_float2(0.f, 0.f);
+                q.IE = fmaf(q.GJ, coupling, fmaf(q.wEE, q.S_E, C::w_E__I_0)) - q.wIE * q.S_I;
+                q.II = fmaf(q.wEI, q.S_E, C::w_I__I_0) - q.S_I;
+                q.rE = rate(fmaf(C::a_E, q.IE, -C::b_E), C::d_E, 1.0f / C::d_E, -C::d_E * LOG2E);
+                q.rI = rate(fmaf(C::a_I, q.II, -C::b_I), C::d_I, 1.0f / C::d_I, -C::d_I * LOG2E);
+                // S += sigma sqrt(dt) xi + dt ((1-S_E) gamma_E r_E - S_E/tau_E), constants folded;
+                // __saturatef clips to [0, 1] and maps NaN to 0 like std::max(0, std::min(S, 1))
+                const float aE = fmaf(-kDtGammaE, q.S_E, kDtGammaE);
+                const float dSE = fmaf(aE, q.rE, fmaf(-kDtInvTauE, q.S_E, SQ * n.x));
+                const float dSI = fmaf(kDtGammaI, q.rI, fmaf(-kDtInvTauI, q.S_I, SQ * n.y));
+                q.S_E = __saturatef(q.S_E + dSE);
+                q.S_I = __saturatef(q.S_I + dSI);
+                if (act) S_buf[(p * 2 + (cur ^ 1)) * LD + j] = q.S_E;
             }
-            bw.step(S_E);
-            if (ts % a.TR == 0) {
+            __syncthreads();
+            cur ^= 1;
+        }
+
+#pragma unroll
+        for (int p = 0; p < P; p++) {
+            if (!live[p]) continue;
+            Slot& q = sl[p];
+            c_cons[p]++;  // this millisecond's noise stage is free again
+            q.bw.step(q.S_E);
+            if (--to_frame[p] == 0) {  // ts % TR == 0
+                to_frame[p] = a.TR;
                 if (act) {
-                    a.bold[((size_t)sim * a.frames + frame) * N + j] = bw.bold();
-                    if (frame >= a.n_vols_remove) {
-                        ext[0] += S_E;
-                        ext[1] += IE;
-                        ext[2] += rE;
-                        ext[3] += S_I;
-                        ext[4] += II;
-                        ext[5] += rI;
+                    a.bold[((size_t)sim[p] * a.frames + frame[p]) * N + j] = q.bw.bold();
+                    if (frame[p] >= a.n_vols_remove) {
+                        double* e = ext + (size_t)p * 6 * blockDim.x + threadIdx.x;
+                        e[0 * blockDim.x] += q.S_E;
+                        e[1 * blockDim.x] += q.IE;
+                        e[2 * blockDim.x] += q.rE;
+                        e[3 * blockDim.x] += q.S_I;
+                        e[4 * blockDim.x] += q.II;
+                        e[5 * blockDim.x] += q.rI;
                     }
                 }
-                frame++;
+                frame[p]++;
             }
-            ts++;
-            if (adjusting) {
-                if (ts >= a.samp_start && ts <= a.samp_end) mean_IE += (double)IE;
-                if (ts == a.samp_end) {
+            ts[p]++;
+            if (adjusting[p]) {
+                if (ts[p] >= a.samp_start && ts[p] <= a.samp_end) q.mean_IE += (double)q.IE;
+                if (ts[p] == a.samp_end) {
                     bool needs = false;
                     if (act) {
-                        const double diff = mean_IE / duration - (double)C::b_a_ratio_E;
+                        const double diff = q.mean_IE / duration - (double)C::b_a_ratio_E;
                         if (fabs(diff + 0.026) > 0.005) {
                             needs = true;
-                            if (trial < a.max_trials) {
+                            if (trial[p] < a.max_trials) {
                                 if (diff < -0.026) {
-                                    wIE -= delta;
-                                    delta = fmaxf(delta - 0.001f, 0.001f);
+                                    q.wIE -= q.delta;
+                                    q.delta = fmaxf(q.delta - 0.001f, 0.001f);
                                 } else {
-                                    wIE += delta;
+                                    q.wIE += q.delta;
                                 }
                             }
                         }
                     }
                     if (__syncthreads_or(needs)) {
-                        if (trial < a.max_trials) {
-                            S_E = 0.001f;
-                            S_I = 0.001f;
-                            bw = BW();
-                            mean_IE = 0.0;
+                        if (trial[p] < a.max_trials) {
+                            q.S_E = q.S_I = 0.001f;
+                            q.bw = BW();
+                            q.mean_IE = 0.0;
 #pragma unroll
-                            for (int q = 0; q < 6; q++) ext[q] = 0.0;
-                            if (act) S_buf[cur * LD + j] = S_E;
-                            ts = 0;
-                            frame = 0;
-                            trial++;
-#pragma unroll
-                            for (int s = 0; s < 10; s++)
-                                nz_next[s] = act ? __ldg(noise2 + (size_t)s * sub_stride + j) : make_float2(0.f, 0.f);
+                            for (int e = 0; e < 6; e++) ext[((size_t)p * 6 + e) * blockDim.x + threadIdx.x] = 0.0;
+                            if (act) S_buf[(p * 2 + cur) * LD + j] = q.S_E;
+                            ts[p] = 0;
+                            frame[p] = 0;
+                            to_frame[p] = 1;
+                            trial[p]++;
+                            // the copies already in flight hold milliseconds after
+                            // the restart point: let them land, then refetch from 0
+                            if (threadIdx.x == 0) s_flag = (int)c_issue[p];
+                            __syncthreads();
+                            const uint32_t in_flight_end = (uint32_t)s_flag;
+                            bool lt = false;
+                            for (; c_cons[p] < in_flight_end; c_cons[p]++) lt |= !wait_copy(p, c_cons[p]);
+                            if (threadIdx.x == 0) ms_next[p] = 0;
+                            if (__syncthreads_or(lt)) timed_out = true;
                         } else {
-                            failed = true;
-                            adjusting = false;
+                            failed[p] = true;
+                            adjusting[p] = false;
                         }
                     } else {
-                        adjusting = false;
+                        adjusting[p] = false;
                     }
                     __syncthreads();
                 }
             }
+            if (ts[p] > a.T) {  // particle done: write it out, take the next one
+                if (act) {
+                    a.wIE_out[(size_t)sim[p] * N + j] = (double)q.wIE;
+                    const double kept = (double)(frame[p] - a.n_vols_remove);
 #pragma unroll
-            for (int s = 0; s < 10; s++) nz[s] = nz_next[s];
+                    for (int e = 0; e < 6; e++)
+                        a.ext[((size_t)sim[p] * 6 + e) * N + j] = ext[((size_t)p * 6 + e) * blockDim.x + threadIdx.x] / kept;
+                }
+                if (threadIdx.x == 0) {
+                    a.trials[sim[p]] = trial[p];
+                    a.failed[sim[p]] = failed[p] ? 1 : 0;
+                }
+                load(p);
+            }
         }
-        if (act) {
-            a.wIE_out[(size_t)sim * N + j] = (double)wIE;
-            const double kept = (double)(frame - a.n_vols_remove);
-#pragma unroll
-            for (int q = 0; q < 6; q++) a.ext[((size_t)sim * 6 + q) * N + j] = ext[q] / kept;
-        }
+        if (timed_out) break;
+    }
+    if (timed_out) {
         if (threadIdx.x == 0) {
-            a.trials[sim] = trial;
-            a.failed[sim] = failed ? 1 : 0;
+            atomicOr(a.status, kStatusTimeout);
+            // bounded wait for this CTA's own copies before the CTA exits
+#pragma unroll
+            for (int p = 0; p < P; p++)
+                for (uint32_t c = c_cons[p]; c < c_issue[p]; c++) wait_copy(p, c);
         }
+        __syncthreads();
     }
 }
 
-template <int K>
+template <int K, int P>
 static cudaError_t launch_fast(const SimArgs& a, int grid, cudaStream_t st) {
     const int threads = ((a.N + 31) / 32) * 32;
-    const size_t smem = (size_t)a.N * 4 * K * sizeof(float) + 2 * 4 * K * sizeof(float) + 16;
+    const size_t smem = (size_t)P * kStages * 10 * a.N * sizeof(float2) + (size_t)a.N * 4 * K * sizeof(float) +
+                        (size_t)P * 2 * 4 * K * sizeof(float) + (size_t)P * 6 * threads * sizeof(double) +
+                        (1 + P * kStages) * sizeof(uint64_t);
     cudaError_t e =
-        cudaFuncSetAttribute(integrate_fast_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(integrate_fast_kernel<K, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    integrate_fast_kernel<K><<<grid, threads, smem, st>>>(a);
+    integrate_fast_kernel<K, P><<<grid, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 
@@ -337,10 +461,21 @@ cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStr
     const int ld = bnm_fast_kmax(a.N);
     if (ld) {
         if (a.sc_ld != ld) return cudaErrorInvalidValue;
-        const int grid = a.n_sims < 2 * num_sms ? a.n_sims : 2 * num_sms;
-        switch (ld / 4) {
-#define BNM_K(K) \
-    case K: return launch_fast<K>(a, grid, st);
+        // particles per CTA.  One, with two CTAs per SM, is the default: at 256
+        // particles of 100 nodes on a B200 two interleaved slots per CTA
+        // measured 1.77x slower than two single-slot CTAs per SM (87.6 vs 152.1
+        // sims/s).  BNM_B200_SLOTS=2 selects the two-slot variant.  CTAs are
+        // persistent over the batch.
+        int P = 1;
+        if (const char* e = std::getenv("BNM_B200_SLOTS")) P = std::atoi(e) == 2 ? 2 : 1;
+        const int per_cta = P;
+        int grid = (a.n_sims + per_cta - 1) / per_cta;
+        const int max_grid = P == 1 ? 2 * num_sms : num_sms;
+        if (grid > max_grid) grid = max_grid;
+        switch ((ld / 4) * 4 + P) {
+#define BNM_K(K)                                          \
+    case K * 4 + 1: return launch_fast<K, 1>(a, grid, st); \
+    case K * 4 + 2: return launch_fast<K, 2>(a, grid, st);
             BNM_K(4) BNM_K(8) BNM_K(12) BNM_K(16) BNM_K(20) BNM_K(24) BNM_K(28) BNM_K(32)
 #undef BNM_K
             default: return cudaErrorInvalidValue;

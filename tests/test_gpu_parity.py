@@ -91,8 +91,12 @@ def test_fp32_reference_order_matches_float_build(case, golden, port):
     np.testing.assert_allclose(r["fic_penalty"][same], g["ref_pen_f32"][same], atol=3e-2)
 
 
+@pytest.mark.parametrize("slots", ["1", "2"])
 @pytest.mark.parametrize("case", CASES)
-def test_fp32_product_path_within_tolerance_of_fp64(case, golden, port):
+def test_fp32_product_path_within_tolerance_of_fp64(case, slots, golden, port, monkeypatch):
+    """slots: particles integrated per CTA by the register kernel (the launcher
+    picks 1 or 2 from the batch size; forced here to cover both)."""
+    monkeypatch.setenv("BNM_B200_SLOTS", slots)
     g = golden[case]
     with _plan(g, B.PREC_F32, port) as p:
         r = p.run(g["G"], g["wEE"], g["wEI"])
