@@ -308,6 +308,48 @@ def run_b200(args):
     return 0
 
 
+def run_surrogate(args):
+    """Surrogate-screened vs plain CMA-ES (second metric): N=100, 300 s at TR 1 s,
+    window 44 step 1, FIC on; surrogate trained on --train-sims uniform
+    simulations; CMA-ES lambda=64 for 60 generations, screened runs sample 8x
+    lambda and simulate the best lambda by predicted cost.  Prints one JSON
+    line with both runs' best fits and the screened run's time to come within
+    0.01 of the plain run's best, as a fraction of the plain run's wall time."""
+    import bnm_cuda_b200 as B
+    from bnm_cuda_b200 import surrogate as S, synth
+
+    sc = synth.make_sc(N_NODES, 0.3, 0)
+    cfg = B.Config(nodes=N_NODES, max_sims=2048, time_steps=300_000, bold_tr=1000, window_size=WS, window_step=1,
+                   bold_remove_s=REMOVE_S, noise_seed=410)
+    s = cfg.sizes()
+    tcfg = B.Config(**{**cfg.__dict__, "max_sims": 1, "noise_seed": 1})
+    with B.Plan(tcfg, sc, np.zeros(s["n_pairs"]), np.zeros(s["n_fcd"])) as tp:
+        tr = tp.run(2.0, 0.3, 0.2, outputs=("fc", "fcd"))
+    bounds, spec = S.Bounds(), S.spectral_summary(sc)
+    with B.Plan(cfg, sc, tr["fc"][0], tr["fcd"][0]) as plan:
+        mlp, info = S.train_surrogate(plan, bounds, spec, n_train=args.train_sims, seed=0, epochs=args.epochs)
+        plain = S.run_cmaes(plan, bounds, 64, args.generations, seed=1)
+        screen = S.run_cmaes(plan, bounds, 64, args.generations, seed=1, mlp=mlp, spec=spec, oversample=8,
+                             holdout_rmse=info["holdout_rmse"])
+    t_fit, ratio = S.time_to_fit(screen, plain, 0.01)
+    print(json.dumps({
+        "metric": "CMA-ES time-to-fit, surrogate-screened / plain", "value": ratio, "unit": "fraction of plain wall",
+        "higher_is_better": False, "data": "synthetic",
+        "config": {"workload": "cmaes-surrogate-N100-300s-lambda64x8-60gen", "train_sims": args.train_sims,
+                   "generations": args.generations},
+        "plain": {"best": plain["best"], "best_x": plain["best_x"], "wall_s": plain["wall_hist"][-1],
+                  "simulations": plain["simulations"], "best_hist": [round(b, 4) for b in plain["best_hist"]]},
+        "screened": {"best": screen["best"], "best_x": screen["best_x"], "wall_s": screen["wall_hist"][-1],
+                     "time_to_fit_s": t_fit, "simulations": screen["simulations"],
+                     "screened_generations": screen["screened_generations"],
+                     "best_hist": [round(b, 4) for b in screen["best_hist"]],
+                     "online_rmse": [round(e, 4) for e in screen["online_rmse"]],
+                     "candidate_spread": [round(e, 4) for e in screen["candidate_spread"]]},
+        "surrogate": {k: v for k, v in info.items() if k != "losses"},
+    }))
+    return 0
+
+
 def main():
     global N_SIMS, T_MS, WORKLOAD
     ap = argparse.ArgumentParser()
@@ -315,6 +357,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--workload", default="generation", choices=["generation", "surrogate"],
+                    help="generation: one CMA-ES generation (headline); surrogate: screened vs plain CMA-ES")
+    ap.add_argument("--train-sims", type=int, default=20_000)
+    ap.add_argument("--epochs", type=int, default=60)
+    ap.add_argument("--generations", type=int, default=60)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--particles", type=int, default=N_SIMS, help="profiling knob: particles per GPU")
     ap.add_argument("--model-ms", type=int, default=T_MS, help="profiling knob: model time per simulation")
@@ -324,6 +371,8 @@ def main():
         WORKLOAD = f"profiling-case-N100-{T_MS // 1000}s-x{N_SIMS}"
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "surrogate":
+        return run_surrogate(args)
     return run_b200(args)
 
 

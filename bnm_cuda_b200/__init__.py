@@ -96,6 +96,7 @@ def lib():
         L.bnm_cmaes_samples.argtypes = [vp, vp, vp, vp]
         L.bnm_cmaes_tell.argtypes = [vp, vp, vp]
         L.bnm_cmaes_best.argtypes = [vp, vp, vp]
+        L.bnm_cmaes_set_samples.argtypes = [vp, vp]
         L.bnm_cmaes_state.argtypes = [vp, vp, vp, vp]
         _lib = L
     return _lib
@@ -321,6 +322,12 @@ class CMAES:
         f, r, p = (np.zeros((self.dim, self.lam)) for _ in range(3))
         lib().bnm_cmaes_samples(self._h, _ptr(f), _ptr(r), _ptr(p))
         return f, r, p
+
+    def set_samples(self, raw):
+        """Replace this generation's raw samples ([dim][lambda]) before tell()."""
+        raw = np.ascontiguousarray(raw, dtype=np.float64).reshape(self.dim, self.lam)
+        if lib().bnm_cmaes_set_samples(self._h, _ptr(raw)) != 0:
+            raise BnmError(BNM_EINVAL, "bad samples")
 
     def tell(self, cost):
         pen = np.zeros(self.lam)

@@ -33,6 +33,7 @@ CU = {
     "capi.cu": [],
     "probe.cu": [],
     "noalloc.cu": [],
+    "mlp.cu": [],
 }
 CPP = ["cmaes.cpp"]
 HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h"]

@@ -469,6 +469,16 @@ extern "C" int32_t bnm_cmaes_tell(bnm_cmaes* c, const double* cost, double* pena
     return c->it;
 }
 
+// Replace the current generation's sample points (raw, [dim][lambda]) before
+// tell(): pre-screened candidates drawn by the caller from N(m, sigma^2 C).
+// No counterpart in the reference.
+extern "C" int bnm_cmaes_set_samples(bnm_cmaes* c, const double* raw) {
+    if (!c || !raw) return 1;
+    std::copy(raw, raw + (size_t)c->D * c->lambda, c->Vars.begin());
+    c->make_feasible();
+    return 0;
+}
+
 extern "C" int bnm_cmaes_best(const bnm_cmaes* c, double* x, double* value) {
     if (x) std::copy(c->CBVfeas.begin(), c->CBVfeas.begin() + c->D, x);
     if (value) *value = c->CBVfeas[c->D];

@@ -220,9 +220,33 @@ int bnm_cmaes_samples(const bnm_cmaes *c, double *feasible, double *raw, double 
  * better); computes the boundary penalty (written to penalized, may be NULL)
  * and samples the next generation.  Returns the new iteration counter. */
 int32_t bnm_cmaes_tell(bnm_cmaes *c, const double *cost, double *penalized);
+/* Replace the current samples (raw [dim][lambda]) before bnm_cmaes_tell, e.g.
+ * with surrogate-pre-screened candidates drawn from N(mean, sigma^2 C).  No
+ * counterpart in the reference. */
+int bnm_cmaes_set_samples(bnm_cmaes *c, const double *raw);
 /* Best feasible point [dim] and its value (-cost, the reference's CBVfeas[D]). */
 int bnm_cmaes_best(const bnm_cmaes *c, double *x, double *value);
 int bnm_cmaes_state(const bnm_cmaes *c, double *mean, double *sigma, double *C);
+
+/* ------------------------------------------------------ MLP surrogate
+ * No counterpart in the reference.  A ReLU MLP (in -> hidden x layers -> out)
+ * trained on the device by the library's own kernels (BF16 tensor-core GEMMs
+ * with FP32 accumulation, MSE loss, Adam), used to pre-screen oversampled
+ * CMA-ES candidates.  Inputs / targets are float, row-major [n][dim], already
+ * normalised by the caller.  Flat parameters: per layer W [out][in] then b. */
+typedef struct bnm_mlp bnm_mlp;
+int bnm_mlp_create(int32_t in_dim, int32_t hidden, int32_t layers, int32_t out_dim, int32_t max_batch, uint64_t seed,
+                   int32_t device, bnm_mlp **out);
+void bnm_mlp_destroy(bnm_mlp *mlp);
+int64_t bnm_mlp_num_params(const bnm_mlp *mlp);
+int bnm_mlp_get_params(bnm_mlp *mlp, float *flat);
+int bnm_mlp_set_params(bnm_mlp *mlp, const float *flat);
+/* epochs of shuffled mini-batches (full batches only); loss_per_epoch may be NULL */
+int bnm_mlp_train(bnm_mlp *mlp, const float *X, const float *Y, int32_t n, int32_t epochs, int32_t batch, float lr,
+                  uint64_t shuffle_seed, float *loss_per_epoch);
+int bnm_mlp_predict(bnm_mlp *mlp, const float *X, int32_t n, float *Y);
+/* one batch (n <= max_batch): MSE loss and the gradient of every parameter, no update */
+int bnm_mlp_loss_and_grads(bnm_mlp *mlp, const float *X, const float *Y, int32_t n, float *loss, float *grads);
 
 #ifdef __cplusplus
 }
