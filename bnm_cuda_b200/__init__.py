@@ -27,6 +27,7 @@ LIB_PATH = os.path.join(HERE, "libbnm_b200.so")
 BNM_OK, BNM_EINVAL, BNM_ENOMEM, BNM_ECUDA, BNM_ETIMEOUT = 0, 1, 2, 3, 4
 PREC_F32, PREC_F64, PREC_F32_REF = 0, 1, 2
 NOISE_PHILOX, NOISE_HOST = 0, 1
+GRAM_F32, GRAM_BF16, GRAM_BF16_SPLIT = 0, 1, 2
 
 _lib = None
 
@@ -45,7 +46,7 @@ class _Config(C.Structure):
                 ("init_delta", C.c_double), ("use_fc_diff", C.c_int32), ("fic_reject_failed", C.c_int32),
                 ("fic_penalty_scale", C.c_double), ("max_cost", C.c_double), ("calculate_fic_penalty", C.c_int32),
                 ("no_fcd", C.c_int32), ("precision", C.c_int32), ("noise_mode", C.c_int32),
-                ("noise_seed", C.c_uint64), ("device", C.c_int32)]
+                ("noise_seed", C.c_uint64), ("device", C.c_int32), ("gram", C.c_int32)]
 
 
 class _Sizes(C.Structure):
@@ -142,6 +143,7 @@ class Config:
     noise_mode: int = NOISE_PHILOX
     noise_seed: int = 410
     device: int = 0
+    gram: int = GRAM_F32
 
     @classmethod
     def from_env(cls, **overrides) -> "Config":

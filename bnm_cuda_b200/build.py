@@ -34,6 +34,7 @@ CU = {
     "probe.cu": [],
     "noalloc.cu": [],
     "mlp.cu": [],
+    "gram_tc.cu": [],
 }
 CPP = ["cmaes.cpp"]
 HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h"]

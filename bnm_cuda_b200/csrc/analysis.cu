@@ -171,23 +171,6 @@ __global__ void __launch_bounds__(256) fc_window_kernel(FcArgs a, const TB* __re
 
 constexpr int kTile = 64, kTk = 16;
 
-__device__ __forceinline__ void window_norm(const double* wsum, int P, double& mean, double& inv_ssd) {
-    mean = wsum[0] / P;
-    const double v = wsum[1] - wsum[0] * mean;
-    inv_ssd = 1.0 / sqrt(v);
-}
-
-// KS bucket of x: c = #emp <= x; also whether x equals emp[c-1].
-__device__ __forceinline__ void ks_bucket(const double* e, int m, double x, int& c, bool& equal) {
-    int lo = 0, hi = m;  // upper_bound
-    while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (e[mid] <= x) lo = mid + 1; else hi = mid;
-    }
-    c = lo;
-    equal = (c > 0) && (e[c - 1] == x);
-}
-
 __global__ void __launch_bounds__(256) fcd_gram_kernel(FcdArgs a) {
     // blockIdx.x: lower-triangular tile index, blockIdx.y: simulation
     int t = blockIdx.x, ta = 0;

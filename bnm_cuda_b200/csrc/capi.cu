@@ -151,6 +151,11 @@ struct bnm_plan {
     double* d_wsum = nullptr;
     unsigned int *d_hist = nullptr, *d_eq = nullptr;
     double *d_cost = nullptr, *d_pen = nullptr, *d_fcc = nullptr, *d_fcdiff = nullptr, *d_ks = nullptr;
+    // tensor-core Grams: BF16 operand tiles (FCD for gram_chunk sims at a time,
+    // FC for all), and the map from the full lower triangle to pair order
+    unsigned char *d_fcd_hi = nullptr, *d_fcd_lo = nullptr, *d_fc_hi = nullptr, *d_fc_lo = nullptr;
+    int* d_tril_map = nullptr;
+    int fcd_rb = 0, fcd_kb = 0, fc_rb = 0, fc_kb = 0, gram_chunk = 0;
     double timings[6] = {0, 0, 0, 0, 0, 0};
     std::vector<void*> allocs;
 };
@@ -191,6 +196,7 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
         return fail(BNM_EINVAL, "host noise needs %lld values (got %lld)", (long long)s.noise_len,
                     (long long)n_host_noise);
     if (cfg->precision < 0 || cfg->precision > 2) return fail(BNM_EINVAL, "unknown precision %d", cfg->precision);
+    if (cfg->gram < 0 || cfg->gram > 2) return fail(BNM_EINVAL, "unknown gram arithmetic %d", cfg->gram);
     for (int i = 0; i < N * N; i++)
         if (!std::isfinite(sc[i])) return fail(BNM_EINVAL, "SC has a non-finite entry at %d", i);
 
@@ -289,6 +295,32 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
     BNM_CUDA_TRY(dalloc(p, &p->d_fcc, n));
     BNM_CUDA_TRY(dalloc(p, &p->d_fcdiff, n));
     BNM_CUDA_TRY(dalloc(p, &p->d_ks, n));
+    if (cfg->gram != BNM_GRAM_F32) {
+        const int parts = cfg->gram == BNM_GRAM_BF16_SPLIT ? 2 : 1;
+        auto blocks = [](int64_t x, int b) { return (int)((x + b - 1) / b); };
+        p->fc_rb = blocks(N, kGramTileRows);
+        p->fc_kb = blocks(s.corr_len, kGramTileK);
+        const size_t fc_bytes = n * p->fc_rb * p->fc_kb * (size_t)kGramTileBytes;
+        BNM_CUDA_TRY(dalloc(p, &p->d_fc_hi, fc_bytes));
+        if (parts == 2) BNM_CUDA_TRY(dalloc(p, &p->d_fc_lo, fc_bytes));
+        std::vector<int> map((size_t)N * (N - 1) / 2, -1);
+        for (size_t q = 0; q < pi.size(); q++) map[(size_t)pi[q] * (pi[q] - 1) / 2 + pj[q]] = (int)q;
+        BNM_CUDA_TRY(dalloc(p, &p->d_tril_map, map.size()));
+        BNM_CUDA_TRY(cudaMemcpy(p->d_tril_map, map.data(), map.size() * 4, cudaMemcpyHostToDevice));
+        if (!cfg->no_fcd) {
+            // FCD operands are large (W x pairs per sim); stage at most 4 GiB of them
+            p->fcd_rb = blocks(s.n_windows, kGramTileRows);
+            p->fcd_kb = blocks(s.n_pairs, kGramTileK);
+            const size_t per_sim = (size_t)p->fcd_rb * p->fcd_kb * kGramTileBytes;
+            const size_t budget = (size_t)4 << 30;
+            p->gram_chunk = (int)std::max<size_t>(1, std::min<size_t>(n, budget / (per_sim * parts)));
+            // BNM_B200_GRAM_CHUNK caps the simulations per staged chunk
+            if (const char* e = std::getenv("BNM_B200_GRAM_CHUNK"))
+                if (std::atoi(e) > 0) p->gram_chunk = std::min(p->gram_chunk, std::atoi(e));
+            BNM_CUDA_TRY(dalloc(p, &p->d_fcd_hi, per_sim * p->gram_chunk));
+            if (parts == 2) BNM_CUDA_TRY(dalloc(p, &p->d_fcd_lo, per_sim * p->gram_chunk));
+        }
+    }
     BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
     return BNM_OK;
 }
@@ -460,9 +492,74 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     fa.wsum = p->d_wsum;
     fa.nan_flag = p->d_nan;
     BNM_CUDA_TRY(bnm_launch_fc_window(fa, st));
+    const int split = c.gram == BNM_GRAM_BF16_SPLIT;
+    if (c.gram != BNM_GRAM_F32) {
+        // FC again as a tensor-core Gram; it replaces the co-moment FC in d_fc
+        OperandArgs oa;
+        std::memset(&oa, 0, sizeof oa);
+        oa.n_sims = n;
+        oa.rows = N;
+        oa.K = s.corr_len;
+        oa.row_blocks = p->fc_rb;
+        oa.kblocks = p->fc_kb;
+        oa.bold = p->d_bold;
+        oa.bold_f64 = p->d_bold64;
+        oa.frames = s.frames;
+        oa.n_vols_remove = s.n_vols_remove;
+        oa.hi = p->d_fc_hi;
+        oa.lo = p->d_fc_lo;
+        BNM_CUDA_TRY(bnm_launch_fc_operand(oa, st));
+        GramArgs ga;
+        std::memset(&ga, 0, sizeof ga);
+        ga.n_sims = n;
+        ga.rows = N;
+        ga.row_blocks = p->fc_rb;
+        ga.kblocks = p->fc_kb;
+        ga.hi = p->d_fc_hi;
+        ga.lo = p->d_fc_lo;
+        ga.out = p->d_fc;
+        ga.tril_map = p->d_tril_map;
+        ga.out_ld = s.n_pairs;
+        ga.nan_flag = p->d_nan;
+        ga.status = p->d_status;
+        BNM_CUDA_TRY(bnm_launch_gram_tc(ga, split, st));
+    }
     BNM_CUDA_TRY(cudaEventRecord(p->ev[3], st));
 
-    if (!c.no_fcd) {
+    if (!c.no_fcd && c.gram != BNM_GRAM_F32) {
+        for (int c0 = 0; c0 < n; c0 += p->gram_chunk) {
+            const int cn = std::min(p->gram_chunk, n - c0);
+            OperandArgs oa;
+            std::memset(&oa, 0, sizeof oa);
+            oa.n_sims = cn;
+            oa.rows = s.n_windows;
+            oa.K = s.n_pairs;
+            oa.row_blocks = p->fcd_rb;
+            oa.kblocks = p->fcd_kb;
+            oa.wfc = p->d_wfc + (size_t)c0 * s.n_windows * s.n_pairs;
+            oa.wsum = p->d_wsum + (size_t)c0 * s.n_windows * 2;
+            oa.hi = p->d_fcd_hi;
+            oa.lo = p->d_fcd_lo;
+            BNM_CUDA_TRY(bnm_launch_fcd_operand(oa, st));
+            GramArgs ga;
+            std::memset(&ga, 0, sizeof ga);
+            ga.n_sims = cn;
+            ga.rows = s.n_windows;
+            ga.row_blocks = p->fcd_rb;
+            ga.kblocks = p->fcd_kb;
+            ga.hi = p->d_fcd_hi;
+            ga.lo = p->d_fcd_lo;
+            ga.out = p->d_fcd + (size_t)c0 * s.n_fcd;
+            ga.out_ld = s.n_fcd;
+            ga.emp_sorted = p->d_emp_sorted;
+            ga.m = p->m;
+            ga.hist = p->d_hist + (size_t)c0 * (p->m + 1);
+            ga.eq = p->d_eq + (size_t)c0 * (p->m + 1);
+            ga.nan_flag = p->d_nan + c0;
+            ga.status = p->d_status;
+            BNM_CUDA_TRY(bnm_launch_gram_tc(ga, split, st));
+        }
+    } else if (!c.no_fcd) {
         FcdArgs da;
         da.n_sims = n;
         da.W = s.n_windows;

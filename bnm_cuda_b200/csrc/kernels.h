@@ -55,6 +55,56 @@ struct GofArgs {
     double* fcd_ks;        // [n]
 };
 
+// Mean and 1/||z - mean|| of one window-FC vector from its pair sums
+// (window_fc_stats, bnm.cu:436-467).
+__device__ __forceinline__ void window_norm(const double* wsum, int P, double& mean, double& inv_ssd) {
+    mean = wsum[0] / P;
+    const double v = wsum[1] - wsum[0] * mean;
+    inv_ssd = 1.0 / sqrt(v);
+}
+
+// KS bucket of x: c = #emp <= x; also whether x equals emp[c-1].
+__device__ __forceinline__ void ks_bucket(const double* e, int m, double x, int& c, bool& equal) {
+    int lo = 0, hi = m;  // upper_bound
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (e[mid] <= x) lo = mid + 1; else hi = mid;
+    }
+    c = lo;
+    equal = (c > 0) && (e[c - 1] == x);
+}
+
+// Tensor-core Gram operands: rows x K values as BF16 tiles of 128 rows x 64 K
+// (16 KB, the tcgen05 K-major SWIZZLE_128B layout), tile (sim, row block,
+// k block) at ((sim * row_blocks + rb) * kblocks + kb) * 16384 bytes.
+constexpr int kGramTileRows = 128, kGramTileK = 64, kGramTileBytes = kGramTileRows * kGramTileK * 2;
+
+struct OperandArgs {
+    int n_sims, rows, K, row_blocks, kblocks;
+    const float* wfc;         // FCD rows: [n][W][P] window FC ...
+    const double* wsum;       // ... and its [n][W][2] pair sums
+    const float* bold;        // FC rows: [n][frames][N] BOLD (FP32 integrators) ...
+    const double* bold_f64;   // ... or FP64 (one of the two)
+    int frames, n_vols_remove;
+    unsigned char* hi;        // bf16(x) tiles
+    unsigned char* lo;        // bf16(x - hi) tiles, split only (else null)
+};
+
+struct GramArgs {
+    int n_sims, rows, row_blocks, kblocks;
+    const unsigned char* hi;  // operand tiles (OperandArgs layout)
+    const unsigned char* lo;  // split only
+    float* out;               // lower triangle i > j: out[sim * out_ld + map(i(i-1)/2 + j)], or null
+    const int* tril_map;      // null: identity; else output index, or -1 to drop the entry
+    long long out_ld;
+    const double* emp_sorted; // KS histogram (FCD) as in FcdArgs, or hist == null
+    int m;
+    unsigned int* hist;
+    unsigned int* eq;
+    int* nan_flag;            // [n]
+    int* status;
+};
+
 struct FicArgs {
     int n_sims, N;
     const double* sc;   // [N][N] (values as the chosen precision rounds them)
@@ -73,6 +123,9 @@ cudaError_t bnm_launch_integrate_exact(const bnm::SimArgs& a, int fp64, int num_
 cudaError_t bnm_launch_fc_window(const bnm::FcArgs& a, cudaStream_t st);
 cudaError_t bnm_launch_fcd(bnm::FcdArgs a, cudaStream_t st);
 cudaError_t bnm_launch_gof(const bnm::GofArgs& a, cudaStream_t st);
+cudaError_t bnm_launch_fcd_operand(const bnm::OperandArgs& a, cudaStream_t st);
+cudaError_t bnm_launch_fc_operand(const bnm::OperandArgs& a, cudaStream_t st);
+cudaError_t bnm_launch_gram_tc(const bnm::GramArgs& a, int split, cudaStream_t st);
 cudaError_t bnm_launch_analytic_fic(const bnm::FicArgs& a, cudaStream_t st);
 cudaError_t bnm_launch_philox(float* out, uint64_t n, uint64_t seed, int num_sms, cudaStream_t st);
 extern "C" int bnm_fast_kmax(int N);

@@ -44,6 +44,13 @@ enum { BNM_PREC_F32 = 0, BNM_PREC_F64 = 1, BNM_PREC_F32_REF = 2 };
  * mt19937 + normal_distribution<float> stream, run_CMAES.cpp:640-657). */
 enum { BNM_NOISE_PHILOX = 0, BNM_NOISE_HOST = 1 };
 
+/* Arithmetic of the FC and FCD Grams (both over rows centred and scaled in
+ * FP64).  F32: FCD on the FP32 SIMT pipe, FC from FP64 co-moments.  BF16 and
+ * BF16_SPLIT: FC and FCD as tcgen05 tensor-core Grams with FP32 accumulation,
+ * operands rounded once to BF16, or split into hi + lo BF16 parts with the
+ * hi.hi + hi.lo + lo.hi products accumulated (error near FP32's). */
+enum { BNM_GRAM_F32 = 0, BNM_GRAM_BF16 = 1, BNM_GRAM_BF16_SPLIT = 2 };
+
 /* Run configuration: the reference's CLI arguments and BNM_* settings. */
 typedef struct bnm_config {
     int32_t nodes;             /* argv[6] */
@@ -70,6 +77,7 @@ typedef struct bnm_config {
     int32_t noise_mode;        /* BNM_NOISE_* */
     uint64_t noise_seed;       /* argv[16] */
     int32_t device;
+    int32_t gram;              /* BNM_GRAM_* (no counterpart in the reference, which runs FP32/FP64 SIMT) */
 } bnm_config;
 
 /* Reference defaults (constants.h:93-116). */

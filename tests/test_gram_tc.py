@@ -1,0 +1,97 @@
+"""Tensor-core (tcgen05) FC and FCD Grams in BF16 and split BF16 against the
+FP64 oracle, through the C ABI.
+
+The three Gram arithmetics run on the same device BOLD (the integrator does
+not depend on the Gram setting, so BOLD must be bit-identical), and each FC /
+FCD entry is compared with the oracle port's FP64 FC and FCD of that BOLD
+(check_fit.cpp:19-134).  Tolerances, absolute on correlations in [-1, 1]:
+
+  F32         FC 1e-6 (FP64 co-moments), FCD 2e-5 (FP32 SIMT Gram)
+  BF16        FC 1e-3, FCD 1e-3 (one BF16 rounding per operand value)
+  BF16_SPLIT  FC 1e-5, FCD 1e-5 (hi + lo parts; partial sums of 128 K
+              drained from the tensor-core accumulator into FP32)
+
+The KS distance fused into the Gram epilogue must equal the oracle's
+two-sample KS of the device's own FCD values (to the last bits of the final
+division), and lie within 1e-2
+(BF16) / 2e-3 (F32, split) of the KS of the FP64 FCD.
+"""
+import numpy as np
+import pytest
+
+import bnm_cuda_b200 as B
+from bnm_cuda_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+# N, T (ms), TR (ms), window size, step, removed s, exc_interhem
+CASES = {
+    # 263 windows: 3 row blocks with a ragged last one; 2450 pairs: 39 K tiles (the ring wraps)
+    "n100_w263": (100, 250000, 720, 44, 1, 30, True),
+    # 160 nodes: 2 FC row blocks, 181 frames: 3 K tiles; 12720 pairs, 54 windows: one diagonal FCD tile
+    "n160_allpairs": (160, 100000, 500, 20, 3, 10, False),
+}
+TOL = {B.GRAM_F32: (1e-6, 2e-5, 2e-3), B.GRAM_BF16: (1e-3, 1e-3, 1e-2), B.GRAM_BF16_SPLIT: (1e-5, 1e-5, 2e-3)}
+NAMES = {B.GRAM_F32: "f32", B.GRAM_BF16: "bf16", B.GRAM_BF16_SPLIT: "bf16x3"}
+
+
+def _run_all(case, n=3):
+    N, T, TR, ws, step, remove, exc = CASES[case]
+    sc = synth.make_sc(N, 0.3, 5)
+    G, wEE, wEI = synth.uniform_params(n, N, seed=11)
+    rng = np.random.default_rng(3)
+    emp_fc = rng.uniform(-0.2, 0.8, synth.n_pairs(N, exc))
+    emp_fcd = rng.uniform(-0.3, 1.0, 4001)
+    res = {}
+    for gram in TOL:
+        cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TR, window_size=ws, window_step=step,
+                       bold_remove_s=remove, exc_interhem=exc, gram=gram)
+        with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+            res[gram] = p.run(G, wEE, wEI, outputs=("bold", "fc", "fcd"))
+    return cfg, emp_fcd, res
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_tensor_core_grams_against_fp64_oracle(case, port):
+    cfg, emp_fcd, res = _run_all(case)
+    N, T, TR, ws, step, remove, exc = CASES[case]
+    nvr = cfg.sizes()["n_vols_remove"]
+    bold = res[B.GRAM_F32]["bold"]
+    errs = {}
+    for gram, r in res.items():
+        np.testing.assert_array_equal(r["bold"], bold)
+    for i in range(len(bold)):
+        kept = bold[i][nvr:]
+        fc64 = port.port_fc_tril(kept, exc=exc)
+        fcd64 = port.port_fcd_tril(kept, step, ws, exc=exc)
+        ks64 = port.port_ks(emp_fcd, fcd64)
+        for gram, r in res.items():
+            e = (np.abs(r["fc"][i] - fc64).max(), np.abs(r["fcd"][i] - fcd64).max(), abs(r["fcd_ks"][i] - ks64))
+            errs[NAMES[gram]] = np.maximum(errs.get(NAMES[gram], 0), e)
+            assert r["fcd_ks"][i] == pytest.approx(port.port_ks(emp_fcd, r["fcd"][i]), abs=1e-12), (NAMES[gram], i)
+    print(case, {k: [f"{x:.2e}" for x in v] for k, v in errs.items()})
+    for gram in res:
+        assert np.all(errs[NAMES[gram]] <= np.array(TOL[gram])), (NAMES[gram], errs[NAMES[gram]])
+
+
+def test_staged_chunks_give_the_same_result(monkeypatch):
+    """FCD operands staged a few simulations at a time (BNM_B200_GRAM_CHUNK)
+    give bit-identical FCD and KS."""
+    N, T, TR, ws, step, remove, exc = CASES["n100_w263"]
+    sc = synth.make_sc(N, 0.3, 5)
+    n = 5
+    G, wEE, wEI = synth.uniform_params(n, N, seed=12)
+    rng = np.random.default_rng(4)
+    emp_fc = rng.uniform(-0.2, 0.8, synth.n_pairs(N, exc))
+    emp_fcd = rng.uniform(-0.3, 1.0, 2000)
+    cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TR, window_size=ws, window_step=step,
+                   bold_remove_s=remove, exc_interhem=exc, gram=B.GRAM_BF16_SPLIT)
+    out = []
+    for chunk in (None, "2"):
+        if chunk:
+            monkeypatch.setenv("BNM_B200_GRAM_CHUNK", chunk)
+        with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+            out.append(p.run(G, wEE, wEI, outputs=("fcd",)))
+    np.testing.assert_array_equal(out[0]["fcd"], out[1]["fcd"])
+    np.testing.assert_array_equal(out[0]["fcd_ks"], out[1]["fcd_ks"])
+    np.testing.assert_array_equal(out[0]["cost"], out[1]["cost"])
