@@ -84,6 +84,7 @@ def lib():
         L.bnm_run.argtypes = [vp, i32, vp, vp, vp, vp, C.POINTER(_BatchOut)]
         L.bnm_analytic_fic.argtypes = [vp, i32, vp, vp, vp, vp, vp]
         L.bnm_last_timings.argtypes = [vp, vp]
+        L.bnm_plan_integrator.argtypes = [vp, vp, vp]
         L.bnm_plan_noise.argtypes = [vp, C.c_int64, C.c_int64, vp]
         L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
         L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
@@ -234,6 +235,13 @@ class Plan:
         t = np.zeros(6)
         _check(lib().bnm_last_timings(self._h, _ptr(t)))
         return dict(zip(["fic", "integrate", "fc_window", "fcd_ks", "gof", "total"], t.tolist()))
+
+    def integrator(self) -> dict:
+        """FP32 integrator shape the autotuner picked for the last batch size."""
+        o, t = np.zeros(5, np.int32), C.c_int32()
+        _check(lib().bnm_plan_integrator(self._h, _ptr(o), C.byref(t)))
+        kind = ["register", "cluster", "reference-order"][int(o[0])]
+        return dict(kind=kind, slots=int(o[1]), csize=int(o[2]), rpw=int(o[3]), kr=int(o[4]), tried=t.value)
 
     def noise(self, offset: int, n: int) -> np.ndarray:
         out = np.zeros(n, np.float32)

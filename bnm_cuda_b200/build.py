@@ -35,9 +35,10 @@ CU = {
     "noalloc.cu": [],
     "mlp.cu": [],
     "gram_tc.cu": [],
+    "integrate_cluster.cu": [],
 }
 CPP = ["cmaes.cpp"]
-HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h"]
+HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h", "fp32_model.cuh"]
 
 
 def _newer(src_paths, out):

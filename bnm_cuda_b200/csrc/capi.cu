@@ -133,7 +133,7 @@ struct bnm_plan {
     bnm_sizes sz;
     int num_sms = 0, kmax = 0, sc_ld = 0, m = 0;
     cudaStream_t st = nullptr;
-    cudaEvent_t ev[6] = {};
+    cudaEvent_t ev[6] = {}, tev[2] = {};
     double emp_fc_mean = 0;
     float* d_sc32 = nullptr;
     double *d_sc64 = nullptr, *d_sc_fic = nullptr;
@@ -156,6 +156,9 @@ struct bnm_plan {
     unsigned char *d_fcd_hi = nullptr, *d_fcd_lo = nullptr, *d_fc_hi = nullptr, *d_fc_lo = nullptr;
     int* d_tril_map = nullptr;
     int fcd_rb = 0, fcd_kb = 0, fc_rb = 0, fc_kb = 0, gram_chunk = 0;
+    // FP32 integrator picked by the autotuner for batches of tuned_n particles
+    IntegratorShape shape{};
+    int tuned_n = 0, n_tried = 0;
     double timings[6] = {0, 0, 0, 0, 0, 0};
     std::vector<void*> allocs;
 };
@@ -173,6 +176,8 @@ extern "C" void bnm_plan_destroy(bnm_plan* p) {
     if (p->st) cudaStreamSynchronize(p->st);
     for (void* a : p->allocs) cudaFree(a);
     for (auto& e : p->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : p->tev)
         if (e) cudaEventDestroy(e);
     if (p->st) cudaStreamDestroy(p->st);
     delete p;
@@ -204,6 +209,7 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
     BNM_CUDA_TRY(cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, cfg->device));
     BNM_CUDA_TRY(cudaStreamCreateWithFlags(&p->st, cudaStreamNonBlocking));
     for (auto& e : p->ev) BNM_CUDA_TRY(cudaEventCreate(&e));
+    for (auto& e : p->tev) BNM_CUDA_TRY(cudaEventCreate(&e));
 
     // SC: FP32 rows padded for the register kernel, FP64 for the exact kernel,
     // and the FIC copy rounded like the chosen precision's u_real.
@@ -393,6 +399,80 @@ static int upload_params(bnm_plan* p, int n, const double* G, const double* w_ee
     return BNM_OK;
 }
 
+// Autotuner of the FP32 integrator: times every candidate shape of
+// bnm_integrator_candidates on this batch size over 200 simulated
+// milliseconds without FIC (the per-millisecond cost does not depend on the
+// model time) and keeps the fastest.  BNM_B200_SHAPE="kind,slots,csize,rpw,kr"
+// forces a shape; BNM_B200_SLOTS forces the register kernel's slots;
+// BNM_B200_TUNE=0 takes the first candidate untimed.
+static int tune_integrator(bnm_plan* p, const SimArgs& a) {
+    const int n = a.n_sims;
+    if (p->tuned_n == n) return BNM_OK;
+    IntegratorShape cand[32];
+    const int nc = bnm_integrator_candidates(a.N, cand, 32);
+    if (nc < 1) return fail(BNM_EINVAL, "no FP32 integrator for %d nodes", a.N);
+    p->shape = cand[0];
+    p->n_tried = 0;
+    if (const char* e = std::getenv("BNM_B200_SHAPE")) {
+        IntegratorShape s{};
+        if (std::sscanf(e, "%d,%d,%d,%d,%d", &s.kind, &s.slots, &s.csize, &s.rpw, &s.kr) != 5)
+            return fail(BNM_EINVAL, "BNM_B200_SHAPE must be kind,slots,csize,rpw,kr");
+        p->shape = s;
+        p->tuned_n = n;
+        return BNM_OK;
+    }
+    const char* slots = std::getenv("BNM_B200_SLOTS");
+    if (slots && p->shape.kind == 0) {
+        p->shape.slots = std::atoi(slots) == 2 ? 2 : 1;
+        p->tuned_n = n;
+        return BNM_OK;
+    }
+    const char* tune = std::getenv("BNM_B200_TUNE");
+    if ((tune && std::atoi(tune) == 0) || nc == 1) {
+        p->tuned_n = n;
+        return BNM_OK;
+    }
+    SimArgs t = a;
+    t.T = std::min(a.T, 200);
+    t.adjust_fic = 0;
+    double best = 1e300;
+    for (int i = 0; i < nc; i++) {
+        float ms = 0.f;
+        bool ok = true;
+        for (int rep = 0; rep < 2 && ok; rep++) {  // the first launch also loads the kernel
+            BNM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, 16, p->st));
+            BNM_CUDA_TRY(cudaEventRecord(p->tev[0], p->st));
+            ok = bnm_launch_integrate_shape(t, cand[i], p->num_sms, p->st) == cudaSuccess;
+            BNM_CUDA_TRY(cudaEventRecord(p->tev[1], p->st));
+        }
+        cudaGetLastError();  // a shape that cannot launch is skipped
+        BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
+        if (!ok) continue;
+        BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->tev[0], p->tev[1]));
+        p->n_tried++;
+        if (ms < best) {
+            best = ms;
+            p->shape = cand[i];
+        }
+    }
+    int status = 0;
+    BNM_CUDA_TRY(cudaMemcpy(&status, p->d_status, 4, cudaMemcpyDeviceToHost));
+    if (status) return fail(BNM_ETIMEOUT, "integrator tuning run reported status %d", status);
+    p->tuned_n = n;
+    return BNM_OK;
+}
+
+extern "C" int bnm_plan_integrator(bnm_plan* p, int32_t* out5, int32_t* n_tried) {
+    if (!p || !out5) return fail(BNM_EINVAL, "null argument");
+    out5[0] = p->shape.kind;
+    out5[1] = p->shape.slots;
+    out5[2] = p->shape.csize;
+    out5[3] = p->shape.rpw;
+    out5[4] = p->shape.kr;
+    if (n_tried) *n_tried = p->n_tried;
+    return BNM_OK;
+}
+
 extern "C" int bnm_analytic_fic(bnm_plan* p, int32_t n, const double* G, const double* w_ee, const double* w_ei,
                                 double* w_ie_out, int32_t* unstable_out) {
     if (!p || n < 1 || n > p->cfg.max_sims) return fail(BNM_EINVAL, "n must be in [1, max_sims]");
@@ -467,8 +547,12 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     a.ext = p->d_ext;
     a.work_counter = p->d_counter;
     a.status = p->d_status;
-    if (c.precision == BNM_PREC_F32)
-        BNM_CUDA_TRY(bnm_launch_integrate_f32(a, p->num_sms, st));
+    if (c.precision == BNM_PREC_F32) {
+        if ((rc = tune_integrator(p, a))) return rc;
+        BNM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, 16, st));
+        BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, st));
+        BNM_CUDA_TRY(bnm_launch_integrate_shape(a, p->shape, p->num_sms, st));
+    }
     else
         BNM_CUDA_TRY(bnm_launch_integrate_exact(a, c.precision == BNM_PREC_F64, p->num_sms, st));
     BNM_CUDA_TRY(cudaEventRecord(p->ev[2], st));

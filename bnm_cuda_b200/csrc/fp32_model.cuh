@@ -1,0 +1,84 @@
+// FP32 model pieces shared by the register integrator (N <= 128) and the
+// cluster integrator (N > 128): firing rate, Balloon-Windkessel in deviation
+// variables, shared-memory addressing and a bounded mbarrier wait.
+#pragma once
+#include "kernels.h"
+
+namespace bnm {
+
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// r = x / (1 - exp(-d x)); for |d x| < 0.1 the quotient is evaluated as
+// (1/d) / P(u) with P(u) = (1 - e^-u)/u truncated after u^4 (rel. err < 2e-8).
+__device__ __forceinline__ float rate(float x, float d, float inv_d, float neg_d_log2e) {
+    const float u = d * x;
+    const float e = ex2_approx(x * neg_d_log2e);
+    float p = fmaf(u, 1.0f / 120.0f, -1.0f / 24.0f);
+    p = fmaf(p, u, 1.0f / 6.0f);
+    p = fmaf(p, u, -0.5f);
+    p = fmaf(p, u, 1.0f);
+    const bool small = fabsf(u) < 0.1f;
+    const float num = small ? inv_d : x;
+    const float den = small ? p : (1.0f - e);
+    return num * rcp_approx(den);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Bounded wait on an mbarrier phase; returns false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long max_iter) {
+    for (long long i = 0; i < max_iter; i++) {
+        uint32_t ok;
+        asm volatile(
+            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// Balloon-Windkessel in deviation variables ft = f-1, nt = nu-1, qt = q-1.
+struct BW {
+    float x = 0.f, ft = 0.f, nt = 0.f, qt = 0.f, lnu = 0.f;  // lnu = log(nu) = log1p(nt)
+    __device__ __forceinline__ void step(float S_E) {
+        typedef Model<float> C;
+        const float L1mr = -0.41551544396166582f;  // ln(1 - rho)
+        const float a1 = C::ialpha - 1.0f;         // exponent of nu in nu^(1/alpha) q / nu
+        x = x + C::model_dt * (S_E - C::kappa * x - C::y * ft);
+        const float ft_new = ft + C::model_dt * x;
+        const float pw = expm1f(C::ialpha * lnu);  // nu^(1/alpha) - 1, old nu
+        const float nt_new = nt + C::model_dt * C::itau * (ft - pw);
+        // f (1 - (1-rho)^(1/f)) / rho - 1, without cancellation:
+        // 1 - (1-rho)^(1/f) - rho = -(1-rho) expm1(ln(1-rho) (1/f - 1))
+        const float h = -(1.0f - C::rho) * expm1f(-L1mr * __fdividef(ft, 1.0f + ft));
+        const float inflow = (h + ft * (C::rho + h)) * (1.0f / C::rho);
+        // nu^(1/alpha - 1) q - 1 with the updated nu
+        const float lnu_new = log1pf(nt_new);
+        const float e = expm1f(a1 * lnu_new);
+        const float outflow = e + qt * (1.0f + e);
+        qt = qt + C::model_dt * C::itau * (inflow - outflow);
+        nt = nt_new;
+        lnu = lnu_new;
+        ft = ft_new;
+    }
+    __device__ __forceinline__ float bold() const {
+        typedef Model<float> C;
+        // V0 (k1 (1-q) + k2 (1 - q/nu) + k3 (1-nu))
+        return C::V_0 * (-C::k1 * qt + C::k2 * (nt - qt) / (1.0f + nt) - C::k3 * nt);
+    }
+};
+
+}  // namespace bnm

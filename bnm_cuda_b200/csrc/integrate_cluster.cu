@@ -1,0 +1,499 @@
+// FP32 integrator for 128 < N <= 512: one thread-block cluster per particle.
+//
+// Same model, time loop, FIC restarts, BOLD and extended outputs as the
+// reference's bnm kernel (bnm.cu:72-315) and CPU path (bnm.cpp:167-290), and
+// the same arithmetic as the register integrator of integrate_fast.cu.  What
+// changes is where SC lives: at N = 400 one SC matrix is 640 KB, more than an
+// SM's registers and shared memory together, so a cluster of C CTAs (C picked
+// by the autotuner) splits it by rows:
+//   * CTA rank c owns nodes [c R, c R + R); warp w of it owns RPW consecutive
+//     nodes.  Lane l holds, for each of those rows, the columns l + 32 k
+//     (k < KC = N/32 rounded up): chunks k < KR in registers as row pairs
+//     for packed FMA (fma.rn.f32x2), the rest in shared memory
+//     (conflict-free, one float2 per lane per row pair and chunk);
+//   * each substep a lane reads its KC entries of S_E once (shared memory),
+//     forms RPW partial row sums, and a butterfly reduce-scatter over the 32
+//     lanes leaves every row's full sum in the 32/RPW lanes l / (32/RPW) ==
+//     row, which update that node redundantly (no divergence);
+//   * the new S_E of a node goes to the S_E buffer of every CTA of the
+//     cluster (distributed shared memory stores, one replica lane per
+//     destination rank), S_E is double buffered, and one cluster barrier
+//     (release / acquire) per substep orders the exchange;
+//   * noise arrives one simulated millisecond ahead through a 4-stage
+//     shared-memory ring of bulk copies (each CTA copies only its own nodes:
+//     ten contiguous runs of R x (E, I) per millisecond), tracked by
+//     mbarriers with bounded waits;
+//   * cluster-wide decisions (a late noise copy, the numerical-FIC restart)
+//     are exchanged as flags through distributed shared memory and read after
+//     a cluster barrier, so every CTA of a cluster takes the same branch and
+//     meets the same barriers.
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include "kernels.h"
+#include "fp32_model.cuh"
+
+namespace bnm {
+namespace {
+
+constexpr int kRing = 4;  // noise ring stages (milliseconds)
+
+__device__ __forceinline__ uint32_t cluster_rank() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ uint32_t cluster_size() {
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+    return r;
+}
+__device__ __forceinline__ void cluster_sync() {
+    asm volatile("barrier.cluster.arrive.release.aligned;\n barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+// shared-memory address of the same variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t map_rank(uint32_t local, uint32_t rank) {
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(local), "r"(rank));
+    return r;
+}
+__device__ __forceinline__ void st_cluster_f32(uint32_t addr, float v) {
+    asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+}
+__device__ __forceinline__ void st_cluster_s32(uint32_t addr, int v) {
+    asm volatile("st.shared::cluster.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
+}
+
+// Shared-memory layout (bytes), in this order:
+//   S      [2][32 KC] float          S_E of every node, double buffered
+//   SCs    [W][RPW/2][KC-KR][32] float2  shared-memory part of the SC slice
+//   ring   [kRing][10][R] float2     noise of the own nodes, per millisecond
+//   ext    [6][W RPW] double         extended-output sums of the own nodes
+//   flags  [32] int                  late[2][8], fic[8]
+//   mbar   [kRing] uint64
+template <int RPW, int KC, int KR>
+struct ClusterLayout {
+    static constexpr int kNP = 32 * KC;
+    __host__ __device__ static size_t sc_bytes(int W) { return (size_t)W * (RPW / 2) * (KC - KR) * 32 * sizeof(float2); }
+    __host__ __device__ static size_t ring_off(int W) { return 2 * kNP * sizeof(float) + sc_bytes(W); }
+    __host__ __device__ static size_t ext_off(int W, int R) { return ring_off(W) + (size_t)kRing * 10 * R * sizeof(float2); }
+    __host__ __device__ static size_t flags_off(int W, int R) { return ext_off(W, R) + (size_t)6 * W * RPW * sizeof(double); }
+    __host__ __device__ static size_t mbar_off(int W, int R) { return flags_off(W, R) + 32 * sizeof(int); }
+    __host__ __device__ static size_t bytes(int W, int R) { return mbar_off(W, R) + kRing * sizeof(uint64_t); }
+};
+
+template <int RPW, int KC, int KR>
+__global__ void integrate_cluster_kernel(SimArgs a, int R) {
+    static_assert(RPW == 4 || RPW == 8 || RPW == 16, "RPW");
+    static_assert(KR >= 0 && KR <= KC, "KR");
+    constexpr int NP = 32 * KC;
+    constexpr int NREP = 32 / RPW;  // lanes holding each row after the reduction
+    constexpr int NPAIR = RPW / 2;
+    constexpr int KS = KC - KR;     // chunks in shared memory
+    typedef Model<float> C;
+    typedef ClusterLayout<RPW, KC, KR> L;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int N = a.N;
+    const int W = blockDim.x >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const uint32_t crank = cluster_rank(), csize = cluster_size();
+    const int sim = blockIdx.x / csize;
+    const int r0 = (int)crank * R;
+    const int r_own = max(0, min(N - r0, R));  // nodes this CTA updates
+
+    float* S_buf = reinterpret_cast<float*>(smem_raw);
+    float2* SCs = reinterpret_cast<float2*>(smem_raw + 2 * NP * sizeof(float));
+    float2* ring = reinterpret_cast<float2*>(smem_raw + L::ring_off(W));
+    double* ext = reinterpret_cast<double*>(smem_raw + L::ext_off(W, R));
+    int* flags = reinterpret_cast<int*>(smem_raw + L::flags_off(W, R));  // late[2][8] at 0, fic[8] at 16, issue at 24
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + L::mbar_off(W, R));
+
+    const int rho = lane / NREP, rep = lane % NREP;
+    const int lr = w * RPW + rho;  // local row (node r0 + lr) this lane updates
+    const int node = r0 + lr;
+    const bool act = lr < r_own;
+    const bool owner = act && rep == 0;  // writes outputs
+    const long long kSpin = 1ll << 26;
+
+    // every CTA of the cluster is running before any distributed shared memory access
+    cluster_sync();
+    if (threadIdx.x == 0) {
+        for (int b = 0; b < kRing; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + b)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int k = threadIdx.x; k < 2 * NP; k += blockDim.x) S_buf[k] = (k % NP) < N ? 0.001f : 0.f;
+    for (int k = threadIdx.x; k < 6 * W * RPW; k += blockDim.x) ext[k] = 0.0;
+    if (threadIdx.x < 32) flags[threadIdx.x] = 0;
+
+    // SC slice: rows r0 + w RPW + 2p (+1), columns k 32 + lane; zero outside the matrix
+    float2 scr[NPAIR][KR > 0 ? KR : 1];
+#pragma unroll
+    for (int p = 0; p < NPAIR; p++) {
+        const int ra = w * RPW + 2 * p, rb = ra + 1;
+#pragma unroll
+        for (int k = 0; k < KC; k++) {
+            const int col = k * 32 + lane;
+            const float va = (ra < r_own && col < N) ? a.sc_f32[(size_t)(r0 + ra) * a.sc_ld + col] : 0.f;
+            const float vb = (rb < r_own && col < N) ? a.sc_f32[(size_t)(r0 + rb) * a.sc_ld + col] : 0.f;
+            if (k < KR)
+                scr[p][k < KR ? k : 0] = make_float2(va, vb);
+            else
+                SCs[((size_t)(w * NPAIR + p) * KS + (k - KR)) * 32 + lane] = make_float2(va, vb);
+        }
+    }
+    // buffers initialised in every CTA before anyone writes remote S_E
+    cluster_sync();
+
+    // per-lane distributed-shared-memory targets: replica `rep` serves ranks rep, rep + NREP, ...
+    const uint32_t s_local = smem_addr(S_buf);
+    const uint32_t flags_local = smem_addr(flags);
+
+    const char* noise_bytes = reinterpret_cast<const char*>(a.noise);
+    const uint32_t run_bytes = (uint32_t)(r_own * sizeof(float2));  // one substep of the own nodes
+    const double duration = (double)(a.samp_end - a.samp_start + 1);
+    const float SQ = C::sigma_model * C::sqrt_dt;
+    const float LOG2E = 1.4426950408889634f;
+    const float kDtGammaE = C::dt * C::gamma_E, kDtInvTauE = C::dt / C::tau_E;
+    const float kDtGammaI = C::dt * C::gamma_I, kDtInvTauI = C::dt / C::tau_I;
+
+    float GJ = (float)a.G[sim] * C::J_NMDA;
+    float wEE = act ? (float)a.wEE[(size_t)sim * N + node] : 0.f;
+    float wEI = act ? (float)a.wEI[(size_t)sim * N + node] : 0.f;
+    float wIE = act ? (float)a.wIE[(size_t)sim * N + node] : 0.f;
+    float delta = (float)a.init_delta;
+    float S_E = 0.001f, S_I = 0.001f, IE = 0.f, II = 0.f, rE = 0.f, rI = 0.f;
+    double mean_IE = 0.0;
+    BW bw;
+    int ts = 0, frame = 0, to_frame = 1, trial = 0, ms_next = 0;
+    bool failed = false, adjusting = a.adjust_fic != 0, timed_out = false;
+    uint32_t c_cons = 0, c_issue = 0;
+    int cur = 0;
+
+    auto wait_copy = [&](uint32_t c) -> bool {
+        return mbar_wait(smem_addr(mbar + c % kRing), (c / kRing) & 1, kSpin);
+    };
+    auto issue = [&]() {  // thread 0: keep up to kRing milliseconds in flight
+        while (c_issue < c_cons + kRing && ms_next <= a.T) {
+            const uint32_t st = c_issue % kRing;
+            const uint32_t bar = smem_addr(mbar + st);
+            if (run_bytes) {
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(10 * run_bytes)
+                             : "memory");
+                for (int sub = 0; sub < 10; sub++)
+                    asm volatile(
+                        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                            smem_addr(ring + ((size_t)st * 10 + sub) * R)),
+                        "l"(noise_bytes + (((size_t)ms_next * 10 + sub) * N + r0) * sizeof(float2)), "r"(run_bytes),
+                        "r"(bar)
+                        : "memory");
+            } else {  // a CTA without nodes still keeps the phase sequence
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+            }
+            c_issue++;
+            ms_next++;
+        }
+    };
+    // flags[slot] of every CTA <- v (threads 0 .. csize-1 each write one rank)
+    auto broadcast_flag = [&](int slot, int v) {
+        if (threadIdx.x < csize) st_cluster_s32(map_rank(flags_local + 4u * slot, threadIdx.x), v);
+    };
+
+    while (ts <= a.T) {
+        if (threadIdx.x == 0) issue();
+        const bool late = __syncthreads_or(!wait_copy(c_cons));
+        const int lslot = (int)(c_cons & 1) * 8;
+        broadcast_flag(lslot + (int)crank, late ? 1 : 0);
+        const float2* nz = ring + (size_t)(c_cons % kRing) * 10 * R + (act ? lr : 0);
+
+#pragma unroll 1
+        for (int sub = 0; sub < 10; sub++) {
+            const float* Sc = S_buf + cur * NP;
+            float s[KC];
+#pragma unroll
+            for (int k = 0; k < KC; k++) s[k] = Sc[k * 32 + lane];
+            float2 acc[NPAIR];
+#pragma unroll
+            for (int p = 0; p < NPAIR; p++) acc[p] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int k = 0; k < KC; k++) {
+                const float2 ss = make_float2(s[k], s[k]);
+#pragma unroll
+                for (int p = 0; p < NPAIR; p++) {
+                    const float2 m = (k < KR) ? scr[p][k < KR ? k : 0]
+                                              : SCs[((size_t)(w * NPAIR + p) * KS + (k - KR)) * 32 + lane];
+                    acc[p] = __ffma2_rn(m, ss, acc[p]);
+                }
+            }
+            // butterfly reduce-scatter: after the step on lane bit b the lane keeps the
+            // half of its rows selected by that bit; the row left is lane / NREP
+            float v[RPW];
+#pragma unroll
+            for (int p = 0; p < NPAIR; p++) {
+                v[2 * p] = acc[p].x;
+                v[2 * p + 1] = acc[p].y;
+            }
+#pragma unroll
+            for (int m = RPW, b = 16; m > 1; m >>= 1, b >>= 1) {
+                const bool hi = (lane & b) != 0;
+#pragma unroll
+                for (int i = 0; i < m / 2; i++) {
+                    const float keep = hi ? v[i + m / 2] : v[i];
+                    const float send = hi ? v[i] : v[i + m / 2];
+                    v[i] = keep + __shfl_xor_sync(0xffffffffu, send, b);
+                }
+            }
+#pragma unroll
+            for (int b = NREP / 2; b >= 1; b >>= 1) v[0] += __shfl_xor_sync(0xffffffffu, v[0], b);
+            const float coupling = v[0];
+
+            const float2 n = act ? nz[(size_t)sub * R] : make_float2(0.f, 0.f);
+            IE = fmaf(GJ, coupling, fmaf(wEE, S_E, C::w_E__I_0)) - wIE * S_I;
+            II = fmaf(wEI, S_E, C::w_I__I_0) - S_I;
+            rE = rate(fmaf(C::a_E, IE, -C::b_E), C::d_E, 1.0f / C::d_E, -C::d_E * LOG2E);
+            rI = rate(fmaf(C::a_I, II, -C::b_I), C::d_I, 1.0f / C::d_I, -C::d_I * LOG2E);
+            const float aE = fmaf(-kDtGammaE, S_E, kDtGammaE);
+            const float dSE = fmaf(aE, rE, fmaf(-kDtInvTauE, S_E, SQ * n.x));
+            const float dSI = fmaf(kDtGammaI, rI, fmaf(-kDtInvTauI, S_I, SQ * n.y));
+            S_E = __saturatef(S_E + dSE);
+            S_I = __saturatef(S_I + dSI);
+            if (act) {
+                const uint32_t dst = s_local + (uint32_t)(((cur ^ 1) * NP + node) * sizeof(float));
+                for (uint32_t t = rep; t < csize; t += NREP) st_cluster_f32(map_rank(dst, t), S_E);
+            }
+            cluster_sync();
+            cur ^= 1;
+        }
+        // every CTA wrote its late flag before the barriers above
+        bool any_late = false;
+        for (uint32_t t = 0; t < csize; t++) any_late |= flags[lslot + t] != 0;
+        if (any_late) {
+            timed_out = true;
+            break;
+        }
+        c_cons++;
+        bw.step(S_E);
+        if (--to_frame == 0) {  // ts % TR == 0
+            to_frame = a.TR;
+            if (owner) {
+                a.bold[((size_t)sim * a.frames + frame) * N + node] = bw.bold();
+                if (frame >= a.n_vols_remove) {
+                    double* e = ext + lr;
+                    const int ld = W * RPW;
+                    e[0 * ld] += S_E;
+                    e[1 * ld] += IE;
+                    e[2 * ld] += rE;
+                    e[3 * ld] += S_I;
+                    e[4 * ld] += II;
+                    e[5 * ld] += rI;
+                }
+            }
+            frame++;
+        }
+        ts++;
+        if (adjusting) {
+            if (ts >= a.samp_start && ts <= a.samp_end) mean_IE += (double)IE;
+            if (ts == a.samp_end) {
+                bool needs = false;
+                if (act) {
+                    const double diff = mean_IE / duration - (double)C::b_a_ratio_E;
+                    if (fabs(diff + 0.026) > 0.005) {
+                        needs = true;
+                        if (trial < a.max_trials) {
+                            if (diff < -0.026) {
+                                wIE -= delta;
+                                delta = fmaxf(delta - 0.001f, 0.001f);
+                            } else {
+                                wIE += delta;
+                            }
+                        }
+                    }
+                }
+                broadcast_flag(16 + (int)crank, __syncthreads_or(needs) ? 1 : 0);
+                cluster_sync();
+                bool any = false;
+                for (uint32_t t = 0; t < csize; t++) any |= flags[16 + t] != 0;
+                if (any) {
+                    if (trial < a.max_trials) {
+                        S_E = S_I = 0.001f;
+                        bw = BW();
+                        mean_IE = 0.0;
+                        if (owner)
+                            for (int e = 0; e < 6; e++) ext[e * W * RPW + lr] = 0.0;
+                        if (act) {
+                            const uint32_t dst = s_local + (uint32_t)((cur * NP + node) * sizeof(float));
+                            for (uint32_t t = rep; t < csize; t += NREP) st_cluster_f32(map_rank(dst, t), S_E);
+                        }
+                        ts = 0;
+                        frame = 0;
+                        to_frame = 1;
+                        trial++;
+                        // copies in flight hold milliseconds after the restart point:
+                        // let them land, then refetch from millisecond 0 (thread 0
+                        // issues, so it publishes how far it got)
+                        if (threadIdx.x == 0) flags[24] = (int)c_issue;
+                        __syncthreads();
+                        const uint32_t in_flight_end = (uint32_t)flags[24];
+                        bool lt = false;
+                        for (; c_cons < in_flight_end; c_cons++) lt |= !wait_copy(c_cons);
+                        ms_next = 0;
+                        if (lt && threadIdx.x == 0) atomicOr(a.status, kStatusTimeout);
+                    } else {
+                        failed = true;
+                        adjusting = false;
+                    }
+                } else {
+                    adjusting = false;
+                }
+                cluster_sync();  // restart S_E visible everywhere; fic flags may be rewritten later
+            }
+        }
+    }
+    if (!timed_out && owner) {
+        a.wIE_out[(size_t)sim * N + node] = (double)wIE;
+        const double kept = (double)(frame - a.n_vols_remove);
+        for (int e = 0; e < 6; e++) a.ext[((size_t)sim * 6 + e) * N + node] = ext[e * W * RPW + lr] / kept;
+    }
+    if (!timed_out && crank == 0 && threadIdx.x == 0) {
+        a.trials[sim] = trial;
+        a.failed[sim] = failed ? 1 : 0;
+    }
+    if (timed_out) {
+        if (threadIdx.x == 0) {
+            atomicOr(a.status, kStatusTimeout);
+            for (uint32_t c = c_cons; c < c_issue; c++) wait_copy(c);  // own copies land before exit
+        }
+        __syncthreads();
+    }
+    cluster_sync();  // no CTA leaves while another may still write its shared memory
+}
+
+// ---------------------------------------------------------------- launch
+
+struct Variant {
+    int rpw, kc, kr;
+    const void* fn;
+    size_t (*bytes)(int W, int R);
+};
+
+template <int RPW, int KC, int KR>
+Variant make_variant() {
+    return {RPW, KC, KR, (const void*)&integrate_cluster_kernel<RPW, KC, KR>, &ClusterLayout<RPW, KC, KR>::bytes};
+}
+
+// KC in 5..16 (N in 129..512); rows per warp 8 or 16; 4 or 8 column chunks in registers
+#define BNM_V(KC) make_variant<8, KC, 4>(), make_variant<8, KC, (KC < 8 ? KC : 8)>(), make_variant<16, KC, 4>()
+const std::vector<Variant>& variants() {
+    static const std::vector<Variant> v = {BNM_V(5),  BNM_V(6),  BNM_V(7),  BNM_V(8),  BNM_V(9),  BNM_V(10),
+                                           BNM_V(11), BNM_V(12), BNM_V(13), BNM_V(14), BNM_V(15), BNM_V(16)};
+    return v;
+}
+#undef BNM_V
+
+}  // namespace
+}  // namespace bnm
+
+using namespace bnm;
+
+// Checks one cluster configuration for node count N and fills its launch
+// shape; returns false when it cannot run (too many threads, registers or
+// shared memory, or no cluster of that size fits).
+extern "C" int bnm_cluster_shape(int N, int csize, int rpw, int kr, int* threads, int* rows, size_t* smem) {
+    if (N <= 0 || N > 512 || (N & 1) || csize < 1 || csize > 8) return 0;
+    const int kc = (N + 31) / 32;
+    for (const Variant& v : variants()) {
+        if (v.rpw != rpw || v.kc != kc || v.kr != kr || v.kr > v.kc) continue;
+        int R = (N + csize - 1) / csize;
+        R += R & 1;  // bulk copies of the own nodes' noise need even node runs
+        if ((csize - 1) * R >= N) return 0;  // a rank without nodes
+        const int W = (R + rpw - 1) / rpw;
+        if (W * 32 > 1024) return 0;
+        // the register file is split over the SM's four partitions, so the
+        // kernel's own limit (not 65536 / registers) bounds the block size
+        cudaFuncAttributes fa;
+        if (cudaFuncGetAttributes(&fa, v.fn) != cudaSuccess) return 0;
+        if (W * 32 > fa.maxThreadsPerBlock) return 0;
+        const size_t sm = v.bytes(W, R);
+        if (sm > 227 * 1024) return 0;
+        *threads = W * 32;
+        *rows = R;
+        *smem = sm;
+        return 1;
+    }
+    return 0;
+}
+
+// Diagnostics of one cluster shape for n_sims particles: out[0] threads,
+// out[1] rows per CTA, out[2] shared-memory bytes, out[3] registers per
+// thread, out[4] the kernel's maximum threads per block, out[5] clusters that
+// can be resident at once (negative: the CUDA error of that query).
+extern "C" int bnm_cluster_probe(int N, int csize, int rpw, int kr, int n_sims, int* out) {
+    for (int i = 0; i < 6; i++) out[i] = 0;
+    int threads = 0, R = 0;
+    size_t smem = 0;
+    const int kc = (N + 31) / 32;
+    const void* fn = nullptr;
+    for (const Variant& v : variants())
+        if (v.rpw == rpw && v.kc == kc && v.kr == kr) fn = v.fn;
+    if (!fn) return 1;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, fn) != cudaSuccess) return 2;
+    out[3] = fa.numRegs;
+    out[4] = fa.maxThreadsPerBlock;
+    if (!bnm_cluster_shape(N, csize, rpw, kr, &threads, &R, &smem)) return 3;
+    out[0] = threads;
+    out[1] = R;
+    out[2] = (int)smem;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return 4;
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3((unsigned)(n_sims * csize));
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg);
+    out[5] = e == cudaSuccess ? clusters : -(int)e;
+    cudaGetLastError();
+    return 0;
+}
+
+cudaError_t bnm_launch_integrate_cluster(const SimArgs& a, int csize, int rpw, int kr, cudaStream_t st) {
+    int threads = 0, R = 0;
+    size_t smem = 0;
+    if (!bnm_cluster_shape(a.N, csize, rpw, kr, &threads, &R, &smem)) return cudaErrorInvalidValue;
+    if (a.sc_ld < a.N) return cudaErrorInvalidValue;
+    const int kc = (a.N + 31) / 32;
+    const void* fn = nullptr;
+    for (const Variant& v : variants())
+        if (v.rpw == rpw && v.kc == kc && v.kr == kr) fn = v.fn;
+    if (!fn) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3((unsigned)(a.n_sims * csize));
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, fn, &cfg);
+    if (e != cudaSuccess) return e;
+    if (clusters < 1) return cudaErrorInvalidConfiguration;
+    void* args[] = {(void*)&a, (void*)&R};
+    return cudaLaunchKernelExC(&cfg, fn, args);
+}

@@ -32,85 +32,11 @@
 //   * FIC sampling and the extended-output sums accumulate in FP64.
 #include <cstdlib>
 #include "kernels.h"
+#include "fp32_model.cuh"
 #define BNM_GENERIC_NS fastgen
 #include "integrate_generic.cuh"
 
 namespace bnm {
-
-__device__ __forceinline__ float ex2_approx(float x) {
-    float y;
-    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float rcp_approx(float x) {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-// r = x / (1 - exp(-d x)); for |d x| < 0.1 the quotient is evaluated as
-// (1/d) / P(u) with P(u) = (1 - e^-u)/u truncated after u^4 (rel. err < 2e-8).
-__device__ __forceinline__ float rate(float x, float d, float inv_d, float neg_d_log2e) {
-    const float u = d * x;
-    const float e = ex2_approx(x * neg_d_log2e);
-    float p = fmaf(u, 1.0f / 120.0f, -1.0f / 24.0f);
-    p = fmaf(p, u, 1.0f / 6.0f);
-    p = fmaf(p, u, -0.5f);
-    p = fmaf(p, u, 1.0f);
-    const bool small = fabsf(u) < 0.1f;
-    const float num = small ? inv_d : x;
-    const float den = small ? p : (1.0f - e);
-    return num * rcp_approx(den);
-}
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-// Bounded wait on an mbarrier phase; returns false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long max_iter) {
-    for (long long i = 0; i < max_iter; i++) {
-        uint32_t ok;
-        asm volatile(
-            "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-            : "=r"(ok)
-            : "r"(bar), "r"(parity)
-            : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-
-// Balloon-Windkessel in deviation variables ft = f-1, nt = nu-1, qt = q-1.
-struct BW {
-    float x = 0.f, ft = 0.f, nt = 0.f, qt = 0.f, lnu = 0.f;  // lnu = log(nu) = log1p(nt)
-    __device__ __forceinline__ void step(float S_E) {
-        typedef Model<float> C;
-        const float L1mr = -0.41551544396166582f;  // ln(1 - rho)
-        const float a1 = C::ialpha - 1.0f;         // exponent of nu in nu^(1/alpha) q / nu
-        x = x + C::model_dt * (S_E - C::kappa * x - C::y * ft);
-        const float ft_new = ft + C::model_dt * x;
-        const float pw = expm1f(C::ialpha * lnu);  // nu^(1/alpha) - 1, old nu
-        const float nt_new = nt + C::model_dt * C::itau * (ft - pw);
-        // f (1 - (1-rho)^(1/f)) / rho - 1, without cancellation:
-        // 1 - (1-rho)^(1/f) - rho = -(1-rho) expm1(ln(1-rho) (1/f - 1))
-        const float h = -(1.0f - C::rho) * expm1f(-L1mr * __fdividef(ft, 1.0f + ft));
-        const float inflow = (h + ft * (C::rho + h)) * (1.0f / C::rho);
-        // nu^(1/alpha - 1) q - 1 with the updated nu
-        const float lnu_new = log1pf(nt_new);
-        const float e = expm1f(a1 * lnu_new);
-        const float outflow = e + qt * (1.0f + e);
-        qt = qt + C::model_dt * C::itau * (inflow - outflow);
-        nt = nt_new;
-        lnu = lnu_new;
-        ft = ft_new;
-    }
-    __device__ __forceinline__ float bold() const {
-        typedef Model<float> C;
-        // V0 (k1 (1-q) + k2 (1 - q/nu) + k3 (1-nu))
-        return C::V_0 * (-C::k1 * qt + C::k2 * (nt - qt) / (1.0f + nt) - C::k3 * nt);
-    }
-};
 
 // Noise ring: the 10 substeps x N nodes x (E, I) floats of one simulated
 // millisecond are contiguous in the table (80 N bytes), so one thread brings a
@@ -454,22 +380,16 @@ extern "C" int bnm_fast_kmax(int N) {
     return 4 * K;
 }
 
-// FP32 launch: the register-SC kernel when N <= 128, else the reference-order
-// kernel in float (SC from shared memory when it fits, else from L2).
-cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStream_t st) {
+// Launches one integrator shape (IntegratorShape in kernels.h).
+cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::IntegratorShape& sh, int num_sms,
+                                       cudaStream_t st) {
     using namespace bnm;
-    const int ld = bnm_fast_kmax(a.N);
-    if (ld) {
-        if (a.sc_ld != ld) return cudaErrorInvalidValue;
-        // particles per CTA.  One, with two CTAs per SM, is the default: at 256
-        // particles of 100 nodes on a B200 two interleaved slots per CTA
-        // measured 1.77x slower than two single-slot CTAs per SM (87.6 vs 152.1
-        // sims/s).  BNM_B200_SLOTS=2 selects the two-slot variant.  CTAs are
-        // persistent over the batch.
-        int P = 1;
-        if (const char* e = std::getenv("BNM_B200_SLOTS")) P = std::atoi(e) == 2 ? 2 : 1;
-        const int per_cta = P;
-        int grid = (a.n_sims + per_cta - 1) / per_cta;
+    if (sh.kind == 0) {
+        const int ld = bnm_fast_kmax(a.N);
+        if (!ld || a.sc_ld != ld || (sh.slots != 1 && sh.slots != 2)) return cudaErrorInvalidValue;
+        // CTAs are persistent over the batch: two per SM with one slot, one with two
+        const int P = sh.slots;
+        int grid = (a.n_sims + P - 1) / P;
         const int max_grid = P == 1 ? 2 * num_sms : num_sms;
         if (grid > max_grid) grid = max_grid;
         switch ((ld / 4) * 4 + P) {
@@ -481,6 +401,8 @@ cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStr
             default: return cudaErrorInvalidValue;
         }
     }
+    if (sh.kind == 1) return bnm_launch_integrate_cluster(a, sh.csize, sh.rpw, sh.kr, st);
+    if (sh.kind != 2) return cudaErrorInvalidValue;
     const int threads = ((a.N + 31) / 32) * 32;
     if (threads > 1024) return cudaErrorInvalidValue;
     size_t smem = 2 * (size_t)threads * sizeof(float);
@@ -493,4 +415,45 @@ cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStr
     const int grid = a.n_sims < 2 * num_sms ? a.n_sims : 2 * num_sms;
     fastgen::integrate_generic_kernel<float><<<grid, threads, smem, st>>>(a, sc_in_smem);
     return cudaGetLastError();
+}
+
+int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max) {
+    using namespace bnm;
+    int n = 0;
+    auto add = [&](IntegratorShape s) {
+        if (n < max) out[n] = s;
+        n++;
+    };
+    if (bnm_fast_kmax(N)) {
+        add({0, 1, 0, 0, 0});
+        add({0, 2, 0, 0, 0});
+        return n < max ? n : max;
+    }
+    const int kc = (N + 31) / 32;
+    const int kr_all = kc < 8 ? kc : 8;
+    const int shapes[3][2] = {{8, 4}, {8, kr_all}, {16, 4}};
+    for (int cs : {1, 2, 4, 8})
+        for (int v = 0; v < 3; v++) {
+            if (v == 1 && kr_all == 4) continue;  // same as {8, 4}
+            int threads, rows;
+            size_t smem;
+            if (bnm_cluster_shape(N, cs, shapes[v][0], shapes[v][1], &threads, &rows, &smem))
+                add({1, 0, cs, shapes[v][0], shapes[v][1]});
+        }
+    add({2, 0, 0, 0, 0});
+    return n < max ? n : max;
+}
+
+// FP32 launch without tuning: the register kernel (one slot, or BNM_B200_SLOTS)
+// when N <= 128, else the first cluster shape that fits, else the
+// reference-order kernel in float.
+cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStream_t st) {
+    using namespace bnm;
+    IntegratorShape c[16];
+    const int n = bnm_integrator_candidates(a.N, c, 16);
+    IntegratorShape s = c[0];
+    if (s.kind == 0)
+        if (const char* e = std::getenv("BNM_B200_SLOTS")) s.slots = std::atoi(e) == 2 ? 2 : 1;
+    (void)n;
+    return bnm_launch_integrate_shape(a, s, num_sms, st);
 }

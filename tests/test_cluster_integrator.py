@@ -1,0 +1,90 @@
+"""The thread-block-cluster FP32 integrator (128 < N <= 512) against the FP64
+oracle port, through the C ABI, in oracle-noise mode (the reference's
+mt19937 stream, bnm.cpp:38-43, fed to both).
+
+Every cluster shape the autotuner can pick is forced once (BNM_B200_SHAPE):
+1, 2, 4 and 8 CTAs per particle, 8 or 16 nodes per warp, and SC column chunks
+in registers only or split between registers and shared memory.  Bar, as for
+the register kernel (N <= 128): on particles whose numerical FIC took the same
+decisions, BOLD within 1e-3 of its range, FC / FCD within 1e-3, cost within
+1e-2; wIE equal to the oracle's up to FP32 rounding.
+"""
+import concurrent.futures as cf
+
+import numpy as np
+import pytest
+
+import bnm_cuda_b200 as B
+from bnm_cuda_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+# N, T ms, TR, remove s, window, step, max trials, particles
+SETUPS = {
+    "n160": (160, 15000, 500, 2, 10, 2, 10, 3),
+    "n400": (400, 11000, 500, 2, 6, 2, 2, 2),
+}
+SHAPES = {
+    "n160": ["1,0,1,8,4", "1,0,2,8,5", "1,0,4,16,4", "1,0,8,8,4"],
+    "n400": ["1,0,4,8,4", "1,0,8,8,8", "1,0,8,16,4"],
+}
+
+
+@pytest.fixture(scope="module")
+def cases(port):
+    out = {}
+    for name, (N, T, TR, remove, ws, step, trials, n) in SETUPS.items():
+        sc = synth.make_sc(N, 0.3 if N < 300 else 0.1, 7)
+        G, wEE, wEI = synth.uniform_params(n, N, seed=21, g=(0.5, 2.0))
+        cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TR, window_size=ws, window_step=step,
+                       bold_remove_s=remove, exc_interhem=True, max_fic_trials=trials, noise_mode=B.NOISE_HOST)
+        s = cfg.sizes()
+        noise = port.port_noise(410, s["noise_len"])
+        wie0 = np.stack([port.port_analytic_fic(sc, G[i], wEE[i], wEI[i])[0] for i in range(n)])
+
+        def one(i):
+            return port.port_integrate(sc, G[i], wEE[i], wEI[i], wie0[i], time_steps=T, bold_tr=TR,
+                                       n_vols_remove=s["n_vols_remove"], noise=noise, max_fic_trials=trials)
+
+        with cf.ThreadPoolExecutor(n) as ex:  # the port releases the GIL
+            ref = list(ex.map(one, range(n)))
+        bold = np.stack([r["bold"] for r in ref])
+        kept = bold[:, s["n_vols_remove"]:]
+        fc = np.stack([port.port_fc_tril(k) for k in kept])
+        fcd = np.stack([port.port_fcd_tril(k, step, ws) for k in kept])
+        rng = np.random.default_rng(5)
+        emp_fc, emp_fcd = rng.uniform(-0.2, 0.8, fc.shape[1]), rng.uniform(-0.3, 1.0, 500)
+        cost = np.array([port.port_gof(k, step, ws, emp_fc, emp_fcd)["cost"] for k in kept])
+        out[name] = dict(cfg=cfg, sc=sc, G=G, wEE=wEE, wEI=wEI, wie0=wie0, noise=noise, bold=bold, fc=fc, fcd=fcd,
+                         cost=cost, emp_fc=emp_fc, emp_fcd=emp_fcd, trials=np.array([r["trials"] for r in ref]),
+                         wIE=np.stack([r["wIE"] for r in ref]))
+    return out
+
+
+@pytest.mark.parametrize("name,shape", [(k, s) for k in SHAPES for s in SHAPES[k]])
+def test_cluster_shape_matches_fp64_oracle(name, shape, cases, monkeypatch):
+    c = cases[name]
+    monkeypatch.setenv("BNM_B200_SHAPE", shape)
+    with B.Plan(c["cfg"], c["sc"], c["emp_fc"], c["emp_fcd"], host_noise=c["noise"]) as p:
+        r = p.run(c["G"], c["wEE"], c["wEI"], c["wie0"] if not c["cfg"].do_fic else None)
+        info = p.integrator()
+    assert info["kind"] == "cluster" and f'1,0,{info["csize"]},{info["rpw"]},{info["kr"]}' == shape
+    same = (r["fic_ntrials"] == c["trials"]) & (np.abs(r["w_ie"] - c["wIE"]).max(1) < 1e-4)
+    assert same.sum() >= 1, (r["fic_ntrials"], c["trials"])
+    span = np.ptp(c["bold"], axis=1, keepdims=True) + 1e-12
+    err = (np.abs(r["bold"] - c["bold"]) / span).max(axis=(1, 2))
+    assert err[same].max() < 1e-3, err
+    np.testing.assert_allclose(r["fc"][same], c["fc"][same], atol=1e-3)
+    np.testing.assert_allclose(r["fcd"][same], c["fcd"][same], atol=1e-3)
+    np.testing.assert_allclose(r["cost"][same], c["cost"][same], atol=1e-2)
+
+
+def test_autotuner_picks_a_timed_cluster_shape(cases):
+    c = cases["n160"]
+    with B.Plan(c["cfg"], c["sc"], c["emp_fc"], c["emp_fcd"], host_noise=c["noise"]) as p:
+        r1 = p.run(c["G"], c["wEE"], c["wEI"])
+        info = p.integrator()
+        r2 = p.run(c["G"], c["wEE"], c["wEI"])  # tuned once per batch size
+        assert p.integrator() == info
+    assert info["kind"] == "cluster" and info["tried"] >= 4, info
+    np.testing.assert_array_equal(r1["cost"], r2["cost"])
