@@ -16,9 +16,12 @@
 //     lanes leaves every row's full sum in the 32/RPW lanes l / (32/RPW) ==
 //     row, which update that node redundantly (no divergence);
 //   * the new S_E of a node goes to the S_E buffer of every CTA of the
-//     cluster (distributed shared memory stores, one replica lane per
-//     destination rank), S_E is double buffered, and one cluster barrier
-//     (release / acquire) per substep orders the exchange;
+//     cluster by asynchronous distributed-shared-memory stores (st.async, one
+//     replica lane per destination rank) that count their bytes on the
+//     destination's mbarrier; S_E is double buffered and a CTA waits only for
+//     its own buffer to fill (no cluster-wide barrier per substep).  A remote
+//     CTA can refill a buffer only after it has this CTA's next S_E, which is
+//     sent after this CTA has read the buffer, so the double buffer is safe;
 //   * noise arrives one simulated millisecond ahead through a 4-stage
 //     shared-memory ring of bulk copies (each CTA copies only its own nodes:
 //     ten contiguous runs of R x (E, I) per millisecond), tracked by
@@ -63,6 +66,13 @@ __device__ __forceinline__ void st_cluster_f32(uint32_t addr, float v) {
 __device__ __forceinline__ void st_cluster_s32(uint32_t addr, int v) {
     asm volatile("st.shared::cluster.s32 [%0], %1;" ::"r"(addr), "r"(v) : "memory");
 }
+// asynchronous remote store that completes 4 bytes of transaction on the
+// destination CTA's mbarrier
+__device__ __forceinline__ void st_async_f32(uint32_t addr, float v, uint32_t bar) {
+    asm volatile("st.async.shared::cluster.mbarrier::complete_tx::bytes.f32 [%0], %1, [%2];" ::"r"(addr), "f"(v),
+                 "r"(bar)
+                 : "memory");
+}
 
 // Shared-memory layout (bytes), in this order:
 //   S      [2][32 KC] float          S_E of every node, double buffered
@@ -70,7 +80,7 @@ __device__ __forceinline__ void st_cluster_s32(uint32_t addr, int v) {
 //   ring   [kRing][10][R] float2     noise of the own nodes, per millisecond
 //   ext    [6][W RPW] double         extended-output sums of the own nodes
 //   flags  [32] int                  late[2][8], fic[8]
-//   mbar   [kRing] uint64
+//   mbar   [kRing + 2] uint64       noise stages, then S_E buffers 0 and 1
 template <int RPW, int KC, int KR>
 struct ClusterLayout {
     static constexpr int kNP = 32 * KC;
@@ -79,7 +89,7 @@ struct ClusterLayout {
     __host__ __device__ static size_t ext_off(int W, int R) { return ring_off(W) + (size_t)kRing * 10 * R * sizeof(float2); }
     __host__ __device__ static size_t flags_off(int W, int R) { return ext_off(W, R) + (size_t)6 * W * RPW * sizeof(double); }
     __host__ __device__ static size_t mbar_off(int W, int R) { return flags_off(W, R) + 32 * sizeof(int); }
-    __host__ __device__ static size_t bytes(int W, int R) { return mbar_off(W, R) + kRing * sizeof(uint64_t); }
+    __host__ __device__ static size_t bytes(int W, int R) { return mbar_off(W, R) + (kRing + 2) * sizeof(uint64_t); }
 };
 
 template <int RPW, int KC, int KR>
@@ -118,8 +128,12 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
     // every CTA of the cluster is running before any distributed shared memory access
     cluster_sync();
     if (threadIdx.x == 0) {
-        for (int b = 0; b < kRing; b++)
+        for (int b = 0; b < kRing + 2; b++)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + b)) : "memory");
+        // buffer 1 receives S_E after the first substep: N values of 4 bytes
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar + kRing + 1)),
+                     "r"(4 * N)
+                     : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int k = threadIdx.x; k < 2 * NP; k += blockDim.x) S_buf[k] = (k % NP) < N ? 0.001f : 0.f;
@@ -169,6 +183,17 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
     bool failed = false, adjusting = a.adjust_fic != 0, timed_out = false;
     uint32_t c_cons = 0, c_issue = 0;
     int cur = 0;
+    // S_E exchange: buffer b's mbarrier (mbar[kRing + b]) completes a phase
+    // when all N values of the next S_E have landed there; ph bit b is the
+    // parity this CTA waits for next.  Buffer 0 starts filled locally.
+    uint32_t ph = 0;
+    bool skip_wait = true;
+    const uint32_t sbar_local = smem_addr(mbar + kRing);
+    auto wait_s = [&](int b) -> bool {
+        const bool ok = mbar_wait(sbar_local + 8u * b, (ph >> b) & 1u, kSpin);
+        ph ^= 1u << b;
+        return ok;
+    };
 
     auto wait_copy = [&](uint32_t c) -> bool {
         return mbar_wait(smem_addr(mbar + c % kRing), (c / kRing) & 1, kSpin);
@@ -201,13 +226,19 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
 
     while (ts <= a.T) {
         if (threadIdx.x == 0) issue();
-        const bool late = __syncthreads_or(!wait_copy(c_cons));
+        bool late = __syncthreads_or(!wait_copy(c_cons));
         const int lslot = (int)(c_cons & 1) * 8;
-        broadcast_flag(lslot + (int)crank, late ? 1 : 0);
         const float2* nz = ring + (size_t)(c_cons % kRing) * 10 * R + (act ? lr : 0);
 
 #pragma unroll 1
         for (int sub = 0; sub < 10; sub++) {
+            if (!skip_wait && !late) late = !wait_s(cur);
+            skip_wait = false;
+            __syncthreads();  // all threads are past this phase: arm the buffer's next one
+            if (threadIdx.x == 0 && !late)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar_local + 8u * cur),
+                             "r"(4 * N)
+                             : "memory");
             const float* Sc = S_buf + cur * NP;
             float s[KC];
 #pragma unroll
@@ -257,14 +288,16 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
             const float dSI = fmaf(kDtGammaI, rI, fmaf(-kDtInvTauI, S_I, SQ * n.y));
             S_E = __saturatef(S_E + dSE);
             S_I = __saturatef(S_I + dSI);
-            if (act) {
+            if (act) {  // to buffer cur^1 of every CTA; its mbarrier counts the bytes
                 const uint32_t dst = s_local + (uint32_t)(((cur ^ 1) * NP + node) * sizeof(float));
-                for (uint32_t t = rep; t < csize; t += NREP) st_cluster_f32(map_rank(dst, t), S_E);
+                const uint32_t bar = sbar_local + 8u * (cur ^ 1);
+                for (uint32_t t = rep; t < csize; t += NREP) st_async_f32(map_rank(dst, t), S_E, map_rank(bar, t));
             }
-            cluster_sync();
             cur ^= 1;
         }
-        // every CTA wrote its late flag before the barriers above
+        // a late noise copy or S_E exchange anywhere stops the whole cluster
+        broadcast_flag(lslot + (int)crank, __syncthreads_or(late) ? 1 : 0);
+        cluster_sync();
         bool any_late = false;
         for (uint32_t t = 0; t < csize; t++) any_late |= flags[lslot + t] != 0;
         if (any_late) {
@@ -320,10 +353,12 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
                         mean_IE = 0.0;
                         if (owner)
                             for (int e = 0; e < 6; e++) ext[e * W * RPW + lr] = 0.0;
-                        if (act) {
-                            const uint32_t dst = s_local + (uint32_t)((cur * NP + node) * sizeof(float));
-                            for (uint32_t t = rep; t < csize; t += NREP) st_cluster_f32(map_rank(dst, t), S_E);
-                        }
+                        // the S_E the next substep would read is in flight: let it land,
+                        // then overwrite the buffer locally with the restart state
+                        bool lt = !wait_s(cur);
+                        skip_wait = true;
+                        __syncthreads();
+                        for (int k = threadIdx.x; k < N; k += blockDim.x) S_buf[cur * NP + k] = 0.001f;
                         ts = 0;
                         frame = 0;
                         to_frame = 1;
@@ -334,7 +369,6 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
                         if (threadIdx.x == 0) flags[24] = (int)c_issue;
                         __syncthreads();
                         const uint32_t in_flight_end = (uint32_t)flags[24];
-                        bool lt = false;
                         for (; c_cons < in_flight_end; c_cons++) lt |= !wait_copy(c_cons);
                         ms_next = 0;
                         if (lt && threadIdx.x == 0) atomicOr(a.status, kStatusTimeout);
@@ -345,7 +379,7 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
                 } else {
                     adjusting = false;
                 }
-                cluster_sync();  // restart S_E visible everywhere; fic flags may be rewritten later
+                cluster_sync();  // fic flags may be rewritten only after every CTA read them
             }
         }
     }
@@ -365,7 +399,10 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
         }
         __syncthreads();
     }
-    cluster_sync();  // no CTA leaves while another may still write its shared memory
+    // the S_E sent at the last substep lands before anyone leaves: no CTA
+    // exits while another may still write its shared memory
+    if (!skip_wait) wait_s(cur);
+    cluster_sync();
 }
 
 // ---------------------------------------------------------------- launch
