@@ -232,8 +232,9 @@ def run_b200(args):
 
     sc, G, wEE, wEI = workload_inputs(rank)
     emp_fc, emp_fcd = make_targets(sc)
+    gram = {"f32": B.GRAM_F32, "bf16": B.GRAM_BF16, "bf16x3": B.GRAM_BF16_SPLIT}[args.gram]
     cfg = B.Config(nodes=N_NODES, max_sims=N_SIMS, time_steps=T_MS, bold_tr=TR, window_size=WS, window_step=STEP,
-                   bold_remove_s=REMOVE_S, noise_seed=410, device=local)
+                   bold_remove_s=REMOVE_S, noise_seed=410, device=local, gram=gram)
     plan = B.Plan(cfg, sc, emp_fc, emp_fcd)
     outputs = ("w_ie",)  # the reference returns corr, fic_penalties, w_IE_fic, FIC_failed, fic_n_trials
     for _ in range(args.warmup):
@@ -246,7 +247,7 @@ def run_b200(args):
             dist.barrier()
 
     barrier()
-    dev_ms, integ_ms, wall, flops = [], [], [], []
+    dev_ms, integ_ms, wall, flops, launches = [], [], [], [], 0
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             t0 = time.perf_counter()
@@ -259,6 +260,7 @@ def run_b200(args):
                 torch.cuda.synchronize()
             wall.append(time.perf_counter() - t0)
             t = plan.timings()
+            launches += plan.gram_timing()["launches"]
             dev_ms.append(t["total"])
             integ_ms.append(t["integrate"])
             subs = 10 * (T_MS + 1) + 100_000 * r["fic_ntrials"].astype(np.float64)
@@ -284,11 +286,12 @@ def run_b200(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": WORKLOAD, "nodes": N, "particles_per_gpu": n, "model_time_ms": T_MS,
                        "tr_ms": TR, "window": WS, "step": STEP, "precision": "f32 integration, f64 FIC/centring",
+                       "gram": args.gram, "integrator": plan.integrator(),
                        "noise": "philox table", "l2": "inputs larger than L2 (3.6 GB noise table, 1.4 GB window FC)",
                        "parallelism": f"particles sharded over {world} GPU(s)"},
             "e2e": {"value": e2e, "unit": "sims/s", "h2d_bytes_per_step": 8 * (n + 2 * n * N),
                     "d2h_bytes_per_step": 8 * n * 5 + 4 * n * 3 + 8 * n * N},
-            "gpu_launches": args.steps * 5,
+            "gpu_launches": launches,
             "roofline": {"bound": "fp32", "kernel": "integrate_fast_kernel", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None,
                          "peak_source": "measured on this GPU by bnm_measure_fp32_peak (packed FP32 FMA chains)",
@@ -350,6 +353,113 @@ def run_surrogate(args):
     return 0
 
 
+def fp64_fc_fcd(bold_kept, ws, step, exc):
+    """FP64 restatement of the reference's FC, window FC and FCD (check_fit.cpp:19-134)
+    for one BOLD series of kept frames [T, N]: pairs i > j row-major (optionally
+    without inter-hemispheric pairs), windows centred ws/2 .. T-1-ws/2 by step."""
+    T, N = bold_kept.shape
+    i, j = np.tril_indices(N, -1)
+    if exc:
+        keep = ~((i < N // 2) ^ (j < N // 2))
+        i, j = i[keep], j[keep]
+    y = bold_kept - bold_kept.mean(0)
+    ss = np.sqrt((y * y).sum(0))
+    fc = (y.T @ y)[i, j] / (ss[i] * ss[j])
+    h = ws // 2
+    centres = range(h, T - h, step)
+    wfc = np.empty((len(centres), len(i)))
+    for k, c in enumerate(centres):
+        yw = bold_kept[c - h:c + h + 1]
+        yw = yw - yw.mean(0)
+        sw = np.sqrt((yw * yw).sum(0))
+        wfc[k] = (yw.T @ yw)[i, j] / (sw[i] * sw[j])
+    z = wfc - wfc.mean(1, keepdims=True)
+    z /= np.sqrt((z * z).sum(1, keepdims=True))
+    a, b = np.tril_indices(len(centres), -1)
+    return fc, (z @ z.T)[a, b]
+
+
+def ks_2samp(x, y):
+    """Two-sample Kolmogorov-Smirnov distance sup |F_x - F_y|."""
+    x, y = np.sort(x), np.sort(y)
+    v = np.concatenate([x, y])
+    return float(np.max(np.abs(np.searchsorted(x, v, "right") / len(x) - np.searchsorted(y, v, "right") / len(y))))
+
+
+def run_precision(args):
+    """Precision stress on FC / FCD: 64 particles, N = 400 (10 % density SC,
+    seed 0), 600 s at TR 0.5 s (1201 frames, none removed), window 44 step 1
+    (1157 windows), all 79,800 pairs.  The batch is integrated once (FP32);
+    its BOLD is then analysed with each Gram arithmetic through
+    bnm_check_fit_bold: FP32 SIMT FCD + FP64 co-moment FC, tcgen05 BF16, and
+    tcgen05 split BF16 (hi + lo).  Errors are against an FP64 restatement of
+    the reference formulas on --check-sims particles: max |error| over FC
+    entries, FCD entries, and of the KS distance to the target FCD."""
+    import bnm_cuda_b200 as B
+    from bnm_cuda_b200 import synth
+
+    N, n, T, TRp, WSp, STEPp = 400, args.particles if args.particles != N_SIMS else 64, 600_000, 500, 44, 1
+    sc = synth.make_sc(N, 0.1, 0)
+    G, wEE, wEI = synth.uniform_params(n, N, 1)
+    cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TRp, window_size=WSp, window_step=STEPp,
+                   bold_remove_s=0, exc_interhem=False, noise_seed=410, gram=B.GRAM_F32)
+    s = cfg.sizes()
+    tcfg = B.Config(**{**cfg.__dict__, "max_sims": 1, "noise_seed": 1})
+    with B.Plan(tcfg, sc, np.zeros(s["n_pairs"]), np.zeros(s["n_fcd"])) as tp:
+        tr = tp.run(2.0, 0.3, 0.2, outputs=("fc", "fcd"))
+    emp_fc, emp_fcd = tr["fc"][0], tr["fcd"][0]
+    out = {}
+    with ClockSampler(0) as clk:
+        with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+            t0 = time.perf_counter()
+            r = p.run(G, wEE, wEI, outputs=("bold", "fc", "fcd"))
+            wall = time.perf_counter() - t0
+            tm = p.timings()
+            integ = p.integrator()
+        kept = r["bold"][:, s["n_vols_remove"]:]
+        out["f32"] = dict(fc=r["fc"], fcd=r["fcd"], ks=r["fcd_ks"], stage_ms=tm, gram=None)
+        for name, gram in (("bf16", B.GRAM_BF16), ("bf16x3", B.GRAM_BF16_SPLIT)):
+            gcfg = B.Config(**{**cfg.__dict__, "gram": gram})
+            with B.Plan(gcfg, sc, emp_fc, emp_fcd) as q:
+                for _ in range(2):  # second call timed (first loads the kernels)
+                    f = q.check_fit_bold(kept)
+                out[name] = dict(fc=f["fc"], fcd=f["fcd"], ks=f["fcd_ks"], stage_ms=q.timings(), gram=q.gram_timing())
+    k = min(args.check_sims, n)
+    ref = [fp64_fc_fcd(kept[i], WSp, STEPp, False) for i in range(k)]
+    ks64 = [ks_2samp(emp_fcd, ref[i][1]) for i in range(k)]
+    W, P = s["n_windows"], s["n_pairs"]
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"bf16_tflops": 1590.0}
+    rb = (W + 127) // 128
+    kpad = ((P + 63) // 64) * 64
+    table = {}
+    for name, o in out.items():
+        e = dict(fc_max_abs_err=max(float(np.abs(o["fc"][i] - ref[i][0]).max()) for i in range(k)),
+                 fcd_max_abs_err=max(float(np.abs(o["fcd"][i] - ref[i][1]).max()) for i in range(k)),
+                 fcd_mean_abs_err=float(np.mean([np.abs(o["fcd"][i] - ref[i][1]).mean() for i in range(k)])),
+                 ks_max_abs_err=max(abs(float(o["ks"][i]) - ks64[i]) for i in range(k)),
+                 fcd_stage_ms=o["stage_ms"]["fcd_ks"])
+        if o["gram"]:
+            prods = 3 if name == "bf16x3" else 1
+            mma_flop = n * rb * (rb + 1) / 2 * 128 * 128 * kpad * 2 * prods
+            ms = o["gram"]["fcd_gram_ms"]
+            e.update(fcd_gram_ms=ms, tensor_tflops=mma_flop / (ms * 1e-3) / 1e12,
+                     tensor_frac=mma_flop / (ms * 1e-3) / 1e12 / peaks["bf16_tflops"],
+                     lower_triangle_tflops=n * W * (W - 1) * P * prods / (ms * 1e-3) / 1e12)
+        table[name] = e
+    print(json.dumps({
+        "metric": "sims/s", "value": n / (tm["total"] / 1e3), "unit": "sims/s", "n_gpus": 1, "steps": 1,
+        "higher_is_better": True, "data": "synthetic", "dtype": "f32 integration; FC/FCD Grams f32 / bf16 / bf16x3",
+        "config": {"workload": "precision-stress-N400-600s-x64", "nodes": N, "particles": n, "model_time_ms": T,
+                   "tr_ms": TRp, "window": WSp, "step": STEPp, "windows": W, "pairs": P, "fcd_entries": s["n_fcd"],
+                   "sc_density": 0.1, "integrator": integ, "checked_particles": k},
+        "wall_s": wall, "stage_ms": tm, "precision": table,
+        "tensor_peak": {"bf16_tflops": peaks["bf16_tflops"], "source": "MEASURED_PEAKS.json (cuBLAS bf16 burst)"},
+        "clocks": clk.summary(),
+    }))
+    return 0
+
+
 def main():
     global N_SIMS, T_MS, WORKLOAD
     ap = argparse.ArgumentParser()
@@ -357,8 +467,12 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="generation", choices=["generation", "surrogate"],
-                    help="generation: one CMA-ES generation (headline); surrogate: screened vs plain CMA-ES")
+    ap.add_argument("--workload", default="generation", choices=["generation", "surrogate", "precision"],
+                    help="generation: one CMA-ES generation (headline); surrogate: screened vs plain CMA-ES; "
+                         "precision: FC/FCD Gram arithmetic against FP64 at N=400")
+    ap.add_argument("--check-sims", type=int, default=4, help="precision: particles checked against FP64")
+    ap.add_argument("--gram", default="bf16x3", choices=["f32", "bf16", "bf16x3"],
+                    help="generation: FC/FCD Gram arithmetic")
     ap.add_argument("--train-sims", type=int, default=20_000)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--generations", type=int, default=60)
@@ -373,6 +487,8 @@ def main():
         return run_reference(args)
     if args.workload == "surrogate":
         return run_surrogate(args)
+    if args.workload == "precision":
+        return run_precision(args)
     return run_b200(args)
 
 

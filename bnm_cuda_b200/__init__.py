@@ -85,6 +85,8 @@ def lib():
         L.bnm_analytic_fic.argtypes = [vp, i32, vp, vp, vp, vp, vp]
         L.bnm_last_timings.argtypes = [vp, vp]
         L.bnm_plan_integrator.argtypes = [vp, vp, vp]
+        L.bnm_check_fit_bold.argtypes = [vp, i32, vp, C.POINTER(_BatchOut)]
+        L.bnm_last_gram.argtypes = [vp, vp, vp]
         L.bnm_plan_noise.argtypes = [vp, C.c_int64, C.c_int64, vp]
         L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
         L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
@@ -144,7 +146,7 @@ class Config:
     noise_mode: int = NOISE_PHILOX
     noise_seed: int = 410
     device: int = 0
-    gram: int = GRAM_F32
+    gram: int = GRAM_BF16_SPLIT
 
     @classmethod
     def from_env(cls, **overrides) -> "Config":
@@ -223,6 +225,25 @@ class Plan:
         _check(lib().bnm_run(self._h, n, _ptr(G), _ptr(wEE), _ptr(wEI), _ptr(wIE), C.byref(o)))
         return res
 
+    def check_fit_bold(self, bold, outputs=("fc", "fcd")) -> dict:
+        """Goodness of fit of given BOLD (check_fit_bold, check_fit.cpp:138-217):
+        ``bold`` [n, corr_len, N] kept frames.  Returns cost, fc_corr, fc_diff,
+        fcd_ks and the requested ``outputs`` (fc, fcd)."""
+        s = self.sizes
+        bold = _d(np.asarray(bold))
+        if bold.ndim != 3 or bold.shape[1:] != (s["corr_len"], self.cfg.nodes):
+            raise ValueError(f"bold must be [n, {s['corr_len']}, {self.cfg.nodes}]")
+        n = bold.shape[0]
+        res = {k: np.zeros(n) for k in ("cost", "fic_penalty", "fc_corr", "fc_diff", "fcd_ks")}
+        shapes = {"fc": (n, s["n_pairs"]), "fcd": (n, s["n_fcd"])}
+        for k in outputs:
+            res[k] = np.zeros(shapes[k])
+        o = _BatchOut()
+        for k, _ in _BatchOut._fields_:
+            setattr(o, k, _ptr(res.get(k)))
+        _check(lib().bnm_check_fit_bold(self._h, n, _ptr(bold), C.byref(o)))
+        return res
+
     def analytic_fic(self, G, wEE, wEI):
         G = _d(np.atleast_1d(G))
         n, N = len(G), self.cfg.nodes
@@ -235,6 +256,13 @@ class Plan:
         t = np.zeros(6)
         _check(lib().bnm_last_timings(self._h, _ptr(t)))
         return dict(zip(["fic", "integrate", "fc_window", "fcd_ks", "gof", "total"], t.tolist()))
+
+    def gram_timing(self) -> dict:
+        """Tensor-core Gram kernel times of the last call (ms) and the number of
+        library kernels it launched."""
+        t, k = np.zeros(2), C.c_int32()
+        _check(lib().bnm_last_gram(self._h, _ptr(t), C.byref(k)))
+        return dict(fc_gram_ms=float(t[0]), fcd_gram_ms=float(t[1]), launches=k.value)
 
     def integrator(self) -> dict:
         """FP32 integrator shape the autotuner picked for the last batch size."""

@@ -72,6 +72,7 @@ extern "C" void bnm_config_default(bnm_config* c) {
     c->noise_mode = BNM_NOISE_PHILOX;
     c->noise_seed = 410;
     c->device = 0;
+    c->gram = BNM_GRAM_BF16_SPLIT;
 }
 
 // helpers.cpp:4-19: ints through atoi; doubles through atof, returned as float.
@@ -160,6 +161,10 @@ struct bnm_plan {
     IntegratorShape shape{};
     int tuned_n = 0, n_tried = 0;
     double timings[6] = {0, 0, 0, 0, 0, 0};
+    // tensor-core Gram kernels alone: one event pair per launch (FC, then each FCD chunk)
+    std::vector<cudaEvent_t> gev;
+    int n_gram = 0, launches = 0;
+    double gram_ms[2] = {0, 0};
     std::vector<void*> allocs;
 };
 
@@ -178,6 +183,8 @@ extern "C" void bnm_plan_destroy(bnm_plan* p) {
     for (auto& e : p->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : p->tev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : p->gev)
         if (e) cudaEventDestroy(e);
     if (p->st) cudaStreamDestroy(p->st);
     delete p;
@@ -326,6 +333,9 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
             BNM_CUDA_TRY(dalloc(p, &p->d_fcd_hi, per_sim * p->gram_chunk));
             if (parts == 2) BNM_CUDA_TRY(dalloc(p, &p->d_fcd_lo, per_sim * p->gram_chunk));
         }
+        const int pairs = 1 + (cfg->no_fcd ? 0 : (int)((n + p->gram_chunk - 1) / std::max(p->gram_chunk, 1)));
+        p->gev.assign(2 * pairs, nullptr);
+        for (auto& e : p->gev) BNM_CUDA_TRY(cudaEventCreate(&e));
     }
     BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
     return BNM_OK;
@@ -486,6 +496,210 @@ extern "C" int bnm_analytic_fic(bnm_plan* p, int32_t n, const double* G, const d
     return BNM_OK;
 }
 
+// FC + window FC (+ tensor-core FC Gram), FCD + KS histogram, goodness of
+// fit, on the plan's BOLD buffer; events 3, 4, 5 close the stages.
+static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
+    const bnm_config& c = p->cfg;
+    const bnm_sizes& s = p->sz;
+    const int N = c.nodes;
+    cudaStream_t st = p->st;
+    p->n_gram = 0;
+    p->launches += 2;  // window FC and goodness of fit
+
+    FcArgs fa;
+    fa.N = N;
+    fa.n_sims = n;
+    fa.frames = s.frames;
+    fa.n_vols_remove = s.n_vols_remove;
+    fa.corr_len = s.corr_len;
+    fa.P = s.n_pairs;
+    fa.pair_i = p->d_pi;
+    fa.pair_j = p->d_pj;
+    fa.W = c.no_fcd ? 0 : s.n_windows;
+    fa.win_len = s.window_len;
+    fa.win_step = c.window_step;
+    fa.bold = p->d_bold;
+    fa.bold_f64 = p->d_bold64;
+    fa.fc = p->d_fc;
+    fa.wfc = p->d_wfc;
+    fa.wsum = p->d_wsum;
+    fa.nan_flag = p->d_nan;
+    BNM_CUDA_TRY(bnm_launch_fc_window(fa, st));
+    const int split = c.gram == BNM_GRAM_BF16_SPLIT;
+    if (c.gram != BNM_GRAM_F32) {
+        // FC again as a tensor-core Gram; it replaces the co-moment FC in d_fc
+        OperandArgs oa;
+        std::memset(&oa, 0, sizeof oa);
+        oa.n_sims = n;
+        oa.rows = N;
+        oa.K = s.corr_len;
+        oa.row_blocks = p->fc_rb;
+        oa.kblocks = p->fc_kb;
+        oa.bold = p->d_bold;
+        oa.bold_f64 = p->d_bold64;
+        oa.frames = s.frames;
+        oa.n_vols_remove = s.n_vols_remove;
+        oa.hi = p->d_fc_hi;
+        oa.lo = p->d_fc_lo;
+        BNM_CUDA_TRY(bnm_launch_fc_operand(oa, st));
+        GramArgs ga;
+        std::memset(&ga, 0, sizeof ga);
+        ga.n_sims = n;
+        ga.rows = N;
+        ga.row_blocks = p->fc_rb;
+        ga.kblocks = p->fc_kb;
+        ga.hi = p->d_fc_hi;
+        ga.lo = p->d_fc_lo;
+        ga.out = p->d_fc;
+        ga.tril_map = p->d_tril_map;
+        ga.out_ld = s.n_pairs;
+        ga.nan_flag = p->d_nan;
+        ga.status = p->d_status;
+        BNM_CUDA_TRY(cudaEventRecord(p->gev[0], st));
+        BNM_CUDA_TRY(bnm_launch_gram_tc(ga, split, st));
+        BNM_CUDA_TRY(cudaEventRecord(p->gev[1], st));
+        p->n_gram = 1;
+        p->launches += 2;
+    }
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[3], st));
+
+    if (!c.no_fcd && c.gram != BNM_GRAM_F32) {
+        for (int c0 = 0; c0 < n; c0 += p->gram_chunk) {
+            const int cn = std::min(p->gram_chunk, n - c0);
+            OperandArgs oa;
+            std::memset(&oa, 0, sizeof oa);
+            oa.n_sims = cn;
+            oa.rows = s.n_windows;
+            oa.K = s.n_pairs;
+            oa.row_blocks = p->fcd_rb;
+            oa.kblocks = p->fcd_kb;
+            oa.wfc = p->d_wfc + (size_t)c0 * s.n_windows * s.n_pairs;
+            oa.wsum = p->d_wsum + (size_t)c0 * s.n_windows * 2;
+            oa.hi = p->d_fcd_hi;
+            oa.lo = p->d_fcd_lo;
+            BNM_CUDA_TRY(bnm_launch_fcd_operand(oa, st));
+            GramArgs ga;
+            std::memset(&ga, 0, sizeof ga);
+            ga.n_sims = cn;
+            ga.rows = s.n_windows;
+            ga.row_blocks = p->fcd_rb;
+            ga.kblocks = p->fcd_kb;
+            ga.hi = p->d_fcd_hi;
+            ga.lo = p->d_fcd_lo;
+            ga.out = p->d_fcd + (size_t)c0 * s.n_fcd;
+            ga.out_ld = s.n_fcd;
+            ga.emp_sorted = p->d_emp_sorted;
+            ga.m = p->m;
+            ga.hist = p->d_hist + (size_t)c0 * (p->m + 1);
+            ga.eq = p->d_eq + (size_t)c0 * (p->m + 1);
+            ga.nan_flag = p->d_nan + c0;
+            ga.status = p->d_status;
+            BNM_CUDA_TRY(cudaEventRecord(p->gev[2 * p->n_gram], st));
+            BNM_CUDA_TRY(bnm_launch_gram_tc(ga, split, st));
+            BNM_CUDA_TRY(cudaEventRecord(p->gev[2 * p->n_gram + 1], st));
+            p->n_gram++;
+            p->launches += 2;
+        }
+    } else if (!c.no_fcd) {
+        FcdArgs da;
+        da.n_sims = n;
+        da.W = s.n_windows;
+        da.P = s.n_pairs;
+        da.wfc = p->d_wfc;
+        da.wsum = p->d_wsum;
+        da.fcd = p->d_fcd;
+        da.n_fcd = s.n_fcd;
+        da.emp_sorted = p->d_emp_sorted;
+        da.m = p->m;
+        da.hist = p->d_hist;
+        da.eq = p->d_eq;
+        da.nan_flag = p->d_nan;
+        BNM_CUDA_TRY(bnm_launch_fcd(da, st));
+        p->launches++;
+    }
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[4], st));
+
+    GofArgs ga;
+    ga.n_sims = n;
+    ga.N = N;
+    ga.P = s.n_pairs;
+    ga.n_fcd = s.n_fcd;
+    ga.m = p->m;
+    ga.fc = p->d_fc;
+    ga.emp_fc = p->d_emp_fc;
+    ga.emp_fc_mean = p->emp_fc_mean;
+    ga.hist = p->d_hist;
+    ga.eq = p->d_eq;
+    ga.valid = p->d_valid;
+    ga.ext = p->d_ext;
+    ga.failed = p->d_failed;
+    ga.nan_flag = p->d_nan;
+    ga.use_fc_diff = c.use_fc_diff;
+    ga.calc_fic_penalty = calc_fic_penalty;
+    ga.fic_reject_failed = c.fic_reject_failed;
+    ga.no_fcd = c.no_fcd;
+    ga.max_cost = c.max_cost;
+    ga.fic_penalty_scale = c.fic_penalty_scale;
+    ga.cost = p->d_cost;
+    ga.fic_penalty = p->d_pen;
+    ga.fc_corr = p->d_fcc;
+    ga.fc_diff = p->d_fcdiff;
+    ga.fcd_ks = p->d_ks;
+    BNM_CUDA_TRY(bnm_launch_gof(ga, st));
+    BNM_CUDA_TRY(cudaEventRecord(p->ev[5], st));
+
+    return BNM_OK;
+}
+
+// Copies the requested outputs back, reads the stage timings and the device
+// status word.
+static int finish(bnm_plan* p, int n, bnm_batch_out* out, bool integrated) {
+    const bnm_config& c = p->cfg;
+    const bnm_sizes& s = p->sz;
+    const int N = c.nodes;
+    cudaStream_t st = p->st;
+    int rc;
+    int status = 0;
+    BNM_CUDA_TRY(cudaMemcpyAsync(&status, p->d_status, 4, cudaMemcpyDeviceToHost, st));
+    if ((rc = d2h(out->cost, p->d_cost, n, st))) return rc;
+    if ((rc = d2h(out->fic_penalty, p->d_pen, n, st))) return rc;
+    if ((rc = d2h(out->fc_corr, p->d_fcc, n, st))) return rc;
+    if ((rc = d2h(out->fc_diff, p->d_fcdiff, n, st))) return rc;
+    if ((rc = d2h(out->fcd_ks, p->d_ks, n, st))) return rc;
+    if (integrated) {
+        if ((rc = d2h(out->w_ie, p->d_wIE_out, (size_t)n * N, st))) return rc;
+        if ((rc = d2h(out->fic_failed, p->d_failed, n, st))) return rc;
+        if ((rc = d2h(out->fic_ntrials, p->d_trials, n, st))) return rc;
+        if ((rc = d2h(out->fic_unstable, p->d_unstable, n, st))) return rc;
+        if ((rc = d2h(out->ext_means, p->d_ext, (size_t)n * 6 * N, st))) return rc;
+    }
+    if (integrated && out->bold) {
+        if (c.precision == BNM_PREC_F64)
+            rc = d2h(out->bold, p->d_bold64, (size_t)n * s.frames * N, st);
+        else
+            rc = f2d(out->bold, p->d_bold, (size_t)n * s.frames * N, st);
+        if (rc) return rc;
+    }
+    if ((rc = f2d(out->fc, p->d_fc, (size_t)n * s.n_pairs, st))) return rc;
+    if (!c.no_fcd && (rc = f2d(out->fcd, p->d_fcd, (size_t)n * s.n_fcd, st))) return rc;
+    BNM_CUDA_TRY(cudaStreamSynchronize(st));
+    float ms;
+    for (int i = 0; i < 5; i++) {
+        BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]));
+        p->timings[i] = ms;
+    }
+    BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->ev[0], p->ev[5]));
+    p->timings[5] = ms;
+    p->gram_ms[0] = p->gram_ms[1] = 0;
+    for (int g = 0; g < p->n_gram; g++) {
+        BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->gev[2 * g], p->gev[2 * g + 1]));
+        p->gram_ms[g == 0 ? 0 : 1] += ms;
+    }
+    if (status & kStatusTimeout) return fail(BNM_ETIMEOUT, "a device wait gave up (status %d)", status);
+    if (status) return fail(BNM_ECUDA, "device status %d", status);
+    return BNM_OK;
+}
+
 extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_ee, const double* w_ei,
                        const double* w_ie, bnm_batch_out* out) {
     if (!p || !out || !G || !w_ee || !w_ei) return fail(BNM_EINVAL, "null argument");
@@ -500,6 +714,7 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     cudaStream_t st = p->st;
     BNM_CUDA_TRY(cudaEventRecord(p->ev[0], st));
     const bool device_fic = c.do_fic && !w_ie;
+    p->launches = device_fic ? 2 : 1;  // analytic FIC, integrator
     if (device_fic) {
         if ((rc = launch_fic(p, n))) return rc;
     } else {
@@ -556,171 +771,55 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     else
         BNM_CUDA_TRY(bnm_launch_integrate_exact(a, c.precision == BNM_PREC_F64, p->num_sms, st));
     BNM_CUDA_TRY(cudaEventRecord(p->ev[2], st));
+    if ((rc = launch_analysis(p, n, c.calculate_fic_penalty))) return rc;
+    return finish(p, n, out, true);
+}
 
-    FcArgs fa;
-    fa.N = N;
-    fa.n_sims = n;
-    fa.frames = s.frames;
-    fa.n_vols_remove = s.n_vols_remove;
-    fa.corr_len = s.corr_len;
-    fa.P = s.n_pairs;
-    fa.pair_i = p->d_pi;
-    fa.pair_j = p->d_pj;
-    fa.W = c.no_fcd ? 0 : s.n_windows;
-    fa.win_len = s.window_len;
-    fa.win_step = c.window_step;
-    fa.bold = p->d_bold;
-    fa.bold_f64 = p->d_bold64;
-    fa.fc = p->d_fc;
-    fa.wfc = p->d_wfc;
-    fa.wsum = p->d_wsum;
-    fa.nan_flag = p->d_nan;
-    BNM_CUDA_TRY(bnm_launch_fc_window(fa, st));
-    const int split = c.gram == BNM_GRAM_BF16_SPLIT;
-    if (c.gram != BNM_GRAM_F32) {
-        // FC again as a tensor-core Gram; it replaces the co-moment FC in d_fc
-        OperandArgs oa;
-        std::memset(&oa, 0, sizeof oa);
-        oa.n_sims = n;
-        oa.rows = N;
-        oa.K = s.corr_len;
-        oa.row_blocks = p->fc_rb;
-        oa.kblocks = p->fc_kb;
-        oa.bold = p->d_bold;
-        oa.bold_f64 = p->d_bold64;
-        oa.frames = s.frames;
-        oa.n_vols_remove = s.n_vols_remove;
-        oa.hi = p->d_fc_hi;
-        oa.lo = p->d_fc_lo;
-        BNM_CUDA_TRY(bnm_launch_fc_operand(oa, st));
-        GramArgs ga;
-        std::memset(&ga, 0, sizeof ga);
-        ga.n_sims = n;
-        ga.rows = N;
-        ga.row_blocks = p->fc_rb;
-        ga.kblocks = p->fc_kb;
-        ga.hi = p->d_fc_hi;
-        ga.lo = p->d_fc_lo;
-        ga.out = p->d_fc;
-        ga.tril_map = p->d_tril_map;
-        ga.out_ld = s.n_pairs;
-        ga.nan_flag = p->d_nan;
-        ga.status = p->d_status;
-        BNM_CUDA_TRY(bnm_launch_gram_tc(ga, split, st));
+// Goodness of fit of given BOLD series (check_fit_bold, check_fit.cpp:138-217,
+// for a batch): bold holds n series of corr_len kept frames x nodes (the
+// frames after n_vols_remove), particle-major.  Same FC / FCD / KS / cost as
+// bnm_run on the plan's configuration and targets; no FIC penalty (there is
+// no r_E series), so cost = 1 - r(FC) (+ |dmean FC|) + KS.
+extern "C" int bnm_check_fit_bold(bnm_plan* p, int32_t n, const double* bold, bnm_batch_out* out) {
+    if (!p || !out || !bold) return fail(BNM_EINVAL, "null argument");
+    if (n < 1 || n > p->cfg.max_sims) return fail(BNM_EINVAL, "n=%d outside [1, max_sims=%d]", n, p->cfg.max_sims);
+    const bnm_config& c = p->cfg;
+    const bnm_sizes& s = p->sz;
+    const int N = c.nodes;
+    BNM_CUDA_TRY(cudaSetDevice(c.device));
+    cudaStream_t st = p->st;
+    const size_t per = (size_t)s.corr_len * N, full = (size_t)s.frames * N;
+    if (c.precision == BNM_PREC_F64) {
+        for (int i = 0; i < n; i++)
+            BNM_CUDA_TRY(cudaMemcpyAsync(p->d_bold64 + i * full + (size_t)s.n_vols_remove * N, bold + i * per,
+                                         per * 8, cudaMemcpyHostToDevice, st));
+    } else {
+        std::vector<float> tmp((size_t)n * per);
+        for (size_t k = 0; k < tmp.size(); k++) tmp[k] = (float)bold[k];
+        for (int i = 0; i < n; i++)
+            BNM_CUDA_TRY(cudaMemcpyAsync(p->d_bold + i * full + (size_t)s.n_vols_remove * N, tmp.data() + i * per,
+                                         per * 4, cudaMemcpyHostToDevice, st));
+        BNM_CUDA_TRY(cudaStreamSynchronize(st));  // tmp goes out of scope
     }
-    BNM_CUDA_TRY(cudaEventRecord(p->ev[3], st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_nan, 0, n * 4, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_failed, 0, n * 4, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_ext, 0, (size_t)n * 6 * N * 8, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_wsum, 0, (size_t)n * std::max(s.n_windows, 1) * 2 * 8, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_hist, 0, (size_t)n * (p->m + 1) * 4, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_eq, 0, (size_t)n * (p->m + 1) * 4, st));
+    for (int e = 0; e < 3; e++) BNM_CUDA_TRY(cudaEventRecord(p->ev[e], st));
+    p->launches = 0;
+    int rc = launch_analysis(p, n, 0);
+    if (rc) return rc;
+    return finish(p, n, out, false);
+}
 
-    if (!c.no_fcd && c.gram != BNM_GRAM_F32) {
-        for (int c0 = 0; c0 < n; c0 += p->gram_chunk) {
-            const int cn = std::min(p->gram_chunk, n - c0);
-            OperandArgs oa;
-            std::memset(&oa, 0, sizeof oa);
-            oa.n_sims = cn;
-            oa.rows = s.n_windows;
-            oa.K = s.n_pairs;
-            oa.row_blocks = p->fcd_rb;
-            oa.kblocks = p->fcd_kb;
-            oa.wfc = p->d_wfc + (size_t)c0 * s.n_windows * s.n_pairs;
-            oa.wsum = p->d_wsum + (size_t)c0 * s.n_windows * 2;
-            oa.hi = p->d_fcd_hi;
-            oa.lo = p->d_fcd_lo;
-            BNM_CUDA_TRY(bnm_launch_fcd_operand(oa, st));
-            GramArgs ga;
-            std::memset(&ga, 0, sizeof ga);
-            ga.n_sims = cn;
-            ga.rows = s.n_windows;
-            ga.row_blocks = p->fcd_rb;
-            ga.kblocks = p->fcd_kb;
-            ga.hi = p->d_fcd_hi;
-            ga.lo = p->d_fcd_lo;
-            ga.out = p->d_fcd + (size_t)c0 * s.n_fcd;
-            ga.out_ld = s.n_fcd;
-            ga.emp_sorted = p->d_emp_sorted;
-            ga.m = p->m;
-            ga.hist = p->d_hist + (size_t)c0 * (p->m + 1);
-            ga.eq = p->d_eq + (size_t)c0 * (p->m + 1);
-            ga.nan_flag = p->d_nan + c0;
-            ga.status = p->d_status;
-            BNM_CUDA_TRY(bnm_launch_gram_tc(ga, split, st));
-        }
-    } else if (!c.no_fcd) {
-        FcdArgs da;
-        da.n_sims = n;
-        da.W = s.n_windows;
-        da.P = s.n_pairs;
-        da.wfc = p->d_wfc;
-        da.wsum = p->d_wsum;
-        da.fcd = p->d_fcd;
-        da.n_fcd = s.n_fcd;
-        da.emp_sorted = p->d_emp_sorted;
-        da.m = p->m;
-        da.hist = p->d_hist;
-        da.eq = p->d_eq;
-        da.nan_flag = p->d_nan;
-        BNM_CUDA_TRY(bnm_launch_fcd(da, st));
-    }
-    BNM_CUDA_TRY(cudaEventRecord(p->ev[4], st));
-
-    GofArgs ga;
-    ga.n_sims = n;
-    ga.N = N;
-    ga.P = s.n_pairs;
-    ga.n_fcd = s.n_fcd;
-    ga.m = p->m;
-    ga.fc = p->d_fc;
-    ga.emp_fc = p->d_emp_fc;
-    ga.emp_fc_mean = p->emp_fc_mean;
-    ga.hist = p->d_hist;
-    ga.eq = p->d_eq;
-    ga.valid = p->d_valid;
-    ga.ext = p->d_ext;
-    ga.failed = p->d_failed;
-    ga.nan_flag = p->d_nan;
-    ga.use_fc_diff = c.use_fc_diff;
-    ga.calc_fic_penalty = c.calculate_fic_penalty;
-    ga.fic_reject_failed = c.fic_reject_failed;
-    ga.no_fcd = c.no_fcd;
-    ga.max_cost = c.max_cost;
-    ga.fic_penalty_scale = c.fic_penalty_scale;
-    ga.cost = p->d_cost;
-    ga.fic_penalty = p->d_pen;
-    ga.fc_corr = p->d_fcc;
-    ga.fc_diff = p->d_fcdiff;
-    ga.fcd_ks = p->d_ks;
-    BNM_CUDA_TRY(bnm_launch_gof(ga, st));
-    BNM_CUDA_TRY(cudaEventRecord(p->ev[5], st));
-
-    int status = 0;
-    BNM_CUDA_TRY(cudaMemcpyAsync(&status, p->d_status, 4, cudaMemcpyDeviceToHost, st));
-    if ((rc = d2h(out->cost, p->d_cost, n, st))) return rc;
-    if ((rc = d2h(out->fic_penalty, p->d_pen, n, st))) return rc;
-    if ((rc = d2h(out->fc_corr, p->d_fcc, n, st))) return rc;
-    if ((rc = d2h(out->fc_diff, p->d_fcdiff, n, st))) return rc;
-    if ((rc = d2h(out->fcd_ks, p->d_ks, n, st))) return rc;
-    if ((rc = d2h(out->w_ie, p->d_wIE_out, (size_t)n * N, st))) return rc;
-    if ((rc = d2h(out->fic_failed, p->d_failed, n, st))) return rc;
-    if ((rc = d2h(out->fic_ntrials, p->d_trials, n, st))) return rc;
-    if ((rc = d2h(out->fic_unstable, p->d_unstable, n, st))) return rc;
-    if ((rc = d2h(out->ext_means, p->d_ext, (size_t)n * 6 * N, st))) return rc;
-    if (out->bold) {
-        if (c.precision == BNM_PREC_F64)
-            rc = d2h(out->bold, p->d_bold64, (size_t)n * s.frames * N, st);
-        else
-            rc = f2d(out->bold, p->d_bold, (size_t)n * s.frames * N, st);
-        if (rc) return rc;
-    }
-    if ((rc = f2d(out->fc, p->d_fc, (size_t)n * s.n_pairs, st))) return rc;
-    if (!c.no_fcd && (rc = f2d(out->fcd, p->d_fcd, (size_t)n * s.n_fcd, st))) return rc;
-    BNM_CUDA_TRY(cudaStreamSynchronize(st));
-    float ms;
-    for (int i = 0; i < 5; i++) {
-        BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]));
-        p->timings[i] = ms;
-    }
-    BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->ev[0], p->ev[5]));
-    p->timings[5] = ms;
-    if (status & kStatusTimeout) return fail(BNM_ETIMEOUT, "a device wait gave up (status %d)", status);
-    if (status) return fail(BNM_ECUDA, "device status %d", status);
+extern "C" int bnm_last_gram(bnm_plan* p, double* ms2, int32_t* launches) {
+    if (!p || !ms2) return fail(BNM_EINVAL, "null argument");
+    ms2[0] = p->gram_ms[0];
+    ms2[1] = p->gram_ms[1];
+    if (launches) *launches = p->launches;
     return BNM_OK;
 }
 

@@ -13,7 +13,9 @@
 // inside the library.  BNM_B200_NOISE=philox switches the noise source from
 // the reference's host stream (mt19937 + normal_distribution<float>) to the
 // device Philox table; BNM_B200_PRECISION=f64|f32ref|f32 (default f32)
-// selects the integrator arithmetic.
+// selects the integrator arithmetic and BNM_B200_GRAM=f32|bf16|bf16x3 the FC /
+// FCD Gram arithmetic (default bf16x3 with f32, f32 with the reference-order
+// modes).
 #include <sys/stat.h>
 
 #include <algorithm>
@@ -291,6 +293,12 @@ int main(int argc, char* argv[]) {
     const char* pe = std::getenv("BNM_B200_PRECISION");
     if (pe && !std::strcmp(pe, "f64")) cfg.precision = BNM_PREC_F64;
     if (pe && !std::strcmp(pe, "f32ref")) cfg.precision = BNM_PREC_F32_REF;
+    // reference-order arithmetic keeps FP64 co-moment FC and the FP32 SIMT FCD
+    if (cfg.precision != BNM_PREC_F32) cfg.gram = BNM_GRAM_F32;
+    const char* ge = std::getenv("BNM_B200_GRAM");
+    if (ge && !std::strcmp(ge, "f32")) cfg.gram = BNM_GRAM_F32;
+    if (ge && !std::strcmp(ge, "bf16")) cfg.gram = BNM_GRAM_BF16;
+    if (ge && !std::strcmp(ge, "bf16x3")) cfg.gram = BNM_GRAM_BF16_SPLIT;
     const char* ne = std::getenv("BNM_B200_NOISE");
     const bool philox = ne && !std::strcmp(ne, "philox");
     cfg.noise_mode = philox ? BNM_NOISE_PHILOX : BNM_NOISE_HOST;

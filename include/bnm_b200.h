@@ -77,7 +77,8 @@ typedef struct bnm_config {
     int32_t noise_mode;        /* BNM_NOISE_* */
     uint64_t noise_seed;       /* argv[16] */
     int32_t device;
-    int32_t gram;              /* BNM_GRAM_* (no counterpart in the reference, which runs FP32/FP64 SIMT) */
+    int32_t gram;              /* BNM_GRAM_* (default BF16_SPLIT; no counterpart in the reference, which
+                                  runs FP32/FP64 SIMT) */
 } bnm_config;
 
 /* Reference defaults (constants.h:93-116). */
@@ -147,6 +148,20 @@ int bnm_analytic_fic(bnm_plan *plan, int32_t n, const double *G, const double *w
 
 /* Time of the last bnm_run on the device, per stage, in ms:
  * [0] analytic FIC, [1] integration, [2] FC + window FC, [3] FCD + KS histogram, [4] GOF, [5] total. */
+/* Device time of the tensor-core Gram kernels alone in the last bnm_run /
+ * bnm_check_fit_bold (ms2[0]: FC Gram, ms2[1]: FCD Gram summed over staged
+ * chunks; 0 with BNM_GRAM_F32) and the number of library kernels that call
+ * launched (*launches).  No counterpart in the reference. */
+int bnm_last_gram(bnm_plan *plan, double *ms2, int32_t *launches);
+
+/* Goodness of fit of given BOLD (check_fit_bold, check_fit.cpp:138-217,
+ * batched): bold = n series of corr_len kept frames (those after
+ * n_vols_remove) x nodes, particle-major.  Computes FC, window FC, FCD, the
+ * KS distance and cost on the device with the plan's configuration, Gram
+ * arithmetic and targets, and fills cost, fc_corr, fc_diff, fcd_ks (and fc,
+ * fcd when set) of *out; no FIC penalty is added (fic_penalty = 0). */
+int bnm_check_fit_bold(bnm_plan *plan, int32_t n, const double *bold, bnm_batch_out *out);
+
 int bnm_last_timings(bnm_plan *plan, double *ms6);
 
 /* FP32 integrator configuration the autotuner picked for the plan's last

@@ -25,9 +25,11 @@ pytestmark = pytest.mark.gpu
 
 def _cfg(g, precision, n=None, noise_mode=B.NOISE_HOST):
     N, T, TR, ws, step, remove, exc, nvr, seed = [int(v) for v in g["meta"]]
+    # the reference-order modes are compared at FP64 level: FP64 co-moment FC, FP32 SIMT FCD
+    gram = B.GRAM_BF16_SPLIT if precision == B.PREC_F32 else B.GRAM_F32
     return B.Config(nodes=N, max_sims=n or len(g["G"]), time_steps=T, bold_tr=TR, window_size=ws, window_step=step,
                     bold_remove_s=remove, exc_interhem=bool(exc), precision=precision, noise_mode=noise_mode,
-                    noise_seed=seed)
+                    noise_seed=seed, gram=gram)
 
 
 def _plan(g, precision, port, noise_mode=B.NOISE_HOST):

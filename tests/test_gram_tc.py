@@ -7,7 +7,10 @@ FCD entry is compared with the oracle port's FP64 FC and FCD of that BOLD
 (check_fit.cpp:19-134).  Tolerances, absolute on correlations in [-1, 1]:
 
   F32         FC 1e-6 (FP64 co-moments), FCD 2e-5 (FP32 SIMT Gram)
-  BF16        FC 1e-3, FCD 1e-3 (one BF16 rounding per operand value)
+  BF16        FC 2e-3, FCD 1e-3 (one BF16 rounding per operand value; FC
+              series dominated by a few frames, e.g. the BOLD onset when no
+              frames are removed, do not average the rounding out, so BF16 FC
+              can exceed 1e-3 and split BF16 is the default)
   BF16_SPLIT  FC 1e-5, FCD 1e-5 (hi + lo parts; partial sums of 128 K
               drained from the tensor-core accumulator into FP32)
 
@@ -31,7 +34,7 @@ CASES = {
     # 160 nodes: 2 FC row blocks, 181 frames: 3 K tiles; 12720 pairs, 54 windows: one diagonal FCD tile
     "n160_allpairs": (160, 100000, 500, 20, 3, 10, False),
 }
-TOL = {B.GRAM_F32: (1e-6, 2e-5, 2e-3), B.GRAM_BF16: (1e-3, 1e-3, 1e-2), B.GRAM_BF16_SPLIT: (1e-5, 1e-5, 2e-3)}
+TOL = {B.GRAM_F32: (1e-6, 2e-5, 2e-3), B.GRAM_BF16: (2e-3, 1e-3, 1e-2), B.GRAM_BF16_SPLIT: (1e-5, 1e-5, 2e-3)}
 NAMES = {B.GRAM_F32: "f32", B.GRAM_BF16: "bf16", B.GRAM_BF16_SPLIT: "bf16x3"}
 
 
@@ -95,3 +98,32 @@ def test_staged_chunks_give_the_same_result(monkeypatch):
     np.testing.assert_array_equal(out[0]["fcd"], out[1]["fcd"])
     np.testing.assert_array_equal(out[0]["fcd_ks"], out[1]["fcd_ks"])
     np.testing.assert_array_equal(out[0]["cost"], out[1]["cost"])
+
+
+def test_check_fit_bold_reproduces_the_batch_and_the_oracle(port):
+    """bnm_check_fit_bold on the BOLD a batch produced gives that batch's FC,
+    FCD, KS and cost (the FIC penalty is a separate output, zero here), and
+    agrees with the oracle's check_fit_bold (check_fit.cpp:138-217) on the
+    same BOLD."""
+    N, T, TR, ws, step, remove, exc = CASES["n100_w263"]
+    sc = synth.make_sc(N, 0.3, 5)
+    n = 3
+    G, wEE, wEI = synth.uniform_params(n, N, seed=13)
+    rng = np.random.default_rng(6)
+    emp_fc = rng.uniform(-0.2, 0.8, synth.n_pairs(N, exc))
+    emp_fcd = rng.uniform(-0.3, 1.0, 3000)
+    for gram in TOL:
+        cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TR, window_size=ws, window_step=step,
+                       bold_remove_s=remove, exc_interhem=exc, gram=gram)
+        nvr = cfg.sizes()["n_vols_remove"]
+        with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+            r = p.run(G, wEE, wEI, outputs=("bold", "fc", "fcd"))
+            f = p.check_fit_bold(r["bold"][:, nvr:])
+        np.testing.assert_array_equal(f["fc"], r["fc"])
+        np.testing.assert_array_equal(f["fcd"], r["fcd"])
+        np.testing.assert_array_equal(f["fcd_ks"], r["fcd_ks"])
+        np.testing.assert_allclose(f["cost"], r["cost"], atol=1e-12)  # the penalty is reported apart
+        assert (f["fic_penalty"] == 0).all()
+        for i in range(n):
+            ref = port.port_gof(r["bold"][i][nvr:], step, ws, emp_fc, emp_fcd, exc=exc)
+            assert f["cost"][i] == pytest.approx(ref["cost"], abs=TOL[gram][2] + 1e-3)

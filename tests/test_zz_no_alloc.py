@@ -19,7 +19,8 @@ def test_noalloc_gof_matches_plan_twice(golden, port):
     g = golden["n20_t25s_tr500"]
     N, T, TR, ws, step, remove, exc, nvr, seed = [int(v) for v in g["meta"]]
     cfg = B.Config(nodes=N, max_sims=len(g["G"]), time_steps=T, bold_tr=TR, window_size=ws, window_step=step,
-                   bold_remove_s=remove, exc_interhem=bool(exc), noise_mode=B.NOISE_HOST)
+                   bold_remove_s=remove, exc_interhem=bool(exc), noise_mode=B.NOISE_HOST,
+                   gram=B.GRAM_F32)  # the allocation-free entry point runs the FP32 SIMT FCD and FP64 FC
     nz = port.port_noise(410, cfg.sizes()["noise_len"])
     with B.Plan(cfg, g["sc"], g["emp_fc"], g["emp_fcd"], host_noise=nz) as p:
         r = p.run(g["G"], g["wEE"], g["wEI"], outputs=("bold",))
