@@ -87,6 +87,11 @@ def lib():
         L.bnm_plan_integrator.argtypes = [vp, vp, vp]
         L.bnm_check_fit_bold.argtypes = [vp, i32, vp, C.POINTER(_BatchOut)]
         L.bnm_last_gram.argtypes = [vp, vp, vp]
+        L.bnm_group_create.argtypes = [vp, i32, C.POINTER(vp)]
+        L.bnm_group_destroy.argtypes = [vp]
+        L.bnm_group_destroy.restype = None
+        L.bnm_group_run.argtypes = [vp, vp, vp, vp, vp, vp]
+        L.bnm_group_last.argtypes = [vp, vp, vp]
         L.bnm_plan_noise.argtypes = [vp, C.c_int64, C.c_int64, vp]
         L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
         L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
@@ -275,6 +280,66 @@ class Plan:
         out = np.zeros(n, np.float32)
         _check(lib().bnm_plan_noise(self._h, offset, n, _ptr(out)))
         return out
+
+
+class Group:
+    """Several plans (subjects) run as one CUDA graph per generation
+    (bnm_group_*): each plan on its own stream, one graph launch, one host
+    synchronisation.  ``run`` takes per-plan (G, wEE, wEI) and returns per-plan
+    dicts of cost, fic_penalty, fc_corr, fc_diff, fcd_ks, w_ie, fic_failed,
+    fic_ntrials, fic_unstable."""
+
+    def __init__(self, plans):
+        self.plans = list(plans)
+        arr = (C.c_void_p * len(self.plans))(*[p._h.value for p in self.plans])
+        h = C.c_void_p()
+        _check(lib().bnm_group_create(arr, len(self.plans), C.byref(h)))
+        self._h = h
+
+    def run(self, params) -> list:
+        k = len(self.plans)
+        if len(params) != k:
+            raise ValueError(f"need {k} parameter sets")
+        keep, res, outs = [], [], (_BatchOut * k)()
+        n = (C.c_int32 * k)()
+        Gp, Ep, Ip = (C.c_void_p * k)(), (C.c_void_p * k)(), (C.c_void_p * k)()
+        for i, (p, (G, wEE, wEI)) in enumerate(zip(self.plans, params)):
+            G = _d(np.atleast_1d(G))
+            m, N = len(G), p.cfg.nodes
+            wEE, wEI = _d(np.broadcast_to(wEE, (m, N))), _d(np.broadcast_to(wEI, (m, N)))
+            keep += [G, wEE, wEI]
+            n[i], Gp[i], Ep[i], Ip[i] = m, _ptr(G), _ptr(wEE), _ptr(wEI)
+            r = {x: np.zeros(m) for x in ("cost", "fic_penalty", "fc_corr", "fc_diff", "fcd_ks")}
+            r["w_ie"] = np.zeros((m, N))
+            for x in ("fic_failed", "fic_ntrials", "fic_unstable"):
+                r[x] = np.zeros(m, np.int32)
+            for f, _ in _BatchOut._fields_:
+                setattr(outs[i], f, _ptr(r.get(f)))
+            res.append(r)
+        _check(lib().bnm_group_run(self._h, n, Gp, Ep, Ip, outs))
+        return res
+
+    def last(self) -> dict:
+        ms, g = C.c_double(), C.c_int32()
+        _check(lib().bnm_group_last(self._h, C.byref(ms), C.byref(g)))
+        return dict(ms=ms.value, graph=bool(g.value))
+
+    def close(self):
+        if self._h:
+            lib().bnm_group_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def measure_fp32_peak(device: int = 0) -> float:

@@ -160,6 +160,12 @@ struct bnm_plan {
     // FP32 integrator picked by the autotuner for batches of tuned_n particles
     IntegratorShape shape{};
     int tuned_n = 0, n_tried = 0;
+    // pinned host staging for graph-captured (group) runs
+    unsigned char* pinned = nullptr;
+    double *io_G = nullptr, *io_wEE = nullptr, *io_wEI = nullptr, *io_cost = nullptr, *io_pen = nullptr,
+           *io_fcc = nullptr, *io_fcdiff = nullptr, *io_ks = nullptr, *io_wie = nullptr;
+    int *io_failed = nullptr, *io_trials = nullptr, *io_unstable = nullptr, *io_status = nullptr;
+    bool capturing = false;
     double timings[6] = {0, 0, 0, 0, 0, 0};
     // tensor-core Gram kernels alone: one event pair per launch (FC, then each FCD chunk)
     std::vector<cudaEvent_t> gev;
@@ -180,6 +186,7 @@ extern "C" void bnm_plan_destroy(bnm_plan* p) {
     cudaSetDevice(p->cfg.device);
     if (p->st) cudaStreamSynchronize(p->st);
     for (void* a : p->allocs) cudaFree(a);
+    if (p->pinned) cudaFreeHost(p->pinned);
     for (auto& e : p->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : p->tev)
@@ -445,6 +452,7 @@ static int tune_integrator(bnm_plan* p, const SimArgs& a) {
     SimArgs t = a;
     t.T = std::min(a.T, 200);
     t.adjust_fic = 0;
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, p->st));
     double best = 1e300;
     for (int i = 0; i < nc; i++) {
         float ms = 0.f;
@@ -494,6 +502,12 @@ extern "C" int bnm_analytic_fic(bnm_plan* p, int32_t n, const double* G, const d
     if ((rc = d2h(unstable_out, p->d_unstable, n, p->st))) return rc;
     BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
     return BNM_OK;
+}
+
+// Stage event: inside a graph capture it must become an event-record node
+// (external record) to time anything when the graph runs.
+static cudaError_t rec(bnm_plan* p, cudaEvent_t e) {
+    return p->capturing ? cudaEventRecordWithFlags(e, p->st, cudaEventRecordExternal) : cudaEventRecord(e, p->st);
 }
 
 // FC + window FC (+ tensor-core FC Gram), FCD + KS histogram, goodness of
@@ -555,13 +569,13 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
         ga.out_ld = s.n_pairs;
         ga.nan_flag = p->d_nan;
         ga.status = p->d_status;
-        BNM_CUDA_TRY(cudaEventRecord(p->gev[0], st));
+        BNM_CUDA_TRY(rec(p, p->gev[0]));
         BNM_CUDA_TRY(bnm_launch_gram_tc(ga, split, st));
-        BNM_CUDA_TRY(cudaEventRecord(p->gev[1], st));
+        BNM_CUDA_TRY(rec(p, p->gev[1]));
         p->n_gram = 1;
         p->launches += 2;
     }
-    BNM_CUDA_TRY(cudaEventRecord(p->ev[3], st));
+    BNM_CUDA_TRY(rec(p, p->ev[3]));
 
     if (!c.no_fcd && c.gram != BNM_GRAM_F32) {
         for (int c0 = 0; c0 < n; c0 += p->gram_chunk) {
@@ -594,9 +608,9 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
             ga.eq = p->d_eq + (size_t)c0 * (p->m + 1);
             ga.nan_flag = p->d_nan + c0;
             ga.status = p->d_status;
-            BNM_CUDA_TRY(cudaEventRecord(p->gev[2 * p->n_gram], st));
+            BNM_CUDA_TRY(rec(p, p->gev[2 * p->n_gram]));
             BNM_CUDA_TRY(bnm_launch_gram_tc(ga, split, st));
-            BNM_CUDA_TRY(cudaEventRecord(p->gev[2 * p->n_gram + 1], st));
+            BNM_CUDA_TRY(rec(p, p->gev[2 * p->n_gram + 1]));
             p->n_gram++;
             p->launches += 2;
         }
@@ -617,7 +631,7 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
         BNM_CUDA_TRY(bnm_launch_fcd(da, st));
         p->launches++;
     }
-    BNM_CUDA_TRY(cudaEventRecord(p->ev[4], st));
+    BNM_CUDA_TRY(rec(p, p->ev[4]));
 
     GofArgs ga;
     ga.n_sims = n;
@@ -646,7 +660,7 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
     ga.fc_diff = p->d_fcdiff;
     ga.fcd_ks = p->d_ks;
     BNM_CUDA_TRY(bnm_launch_gof(ga, st));
-    BNM_CUDA_TRY(cudaEventRecord(p->ev[5], st));
+    BNM_CUDA_TRY(rec(p, p->ev[5]));
 
     return BNM_OK;
 }
@@ -700,6 +714,41 @@ static int finish(bnm_plan* p, int n, bnm_batch_out* out, bool integrated) {
     return BNM_OK;
 }
 
+static SimArgs sim_args(bnm_plan* p, int n) {
+    const bnm_config& c = p->cfg;
+    const bnm_sizes& s = p->sz;
+    SimArgs a;
+    std::memset(&a, 0, sizeof a);
+    a.N = c.nodes;
+    a.n_sims = n;
+    a.T = c.time_steps;
+    a.TR = c.bold_tr;
+    a.frames = s.frames;
+    a.n_vols_remove = s.n_vols_remove;
+    a.adjust_fic = c.do_fic && c.numerical_fic;
+    a.max_trials = c.max_fic_trials;
+    a.samp_start = c.i_sampling_start;
+    a.samp_end = c.i_sampling_end;
+    a.init_delta = c.init_delta;
+    a.G = p->d_G;
+    a.wEE = p->d_wEE;
+    a.wEI = p->d_wEI;
+    a.wIE = p->d_wIE;
+    a.noise = p->d_noise;
+    a.sc_f32 = p->d_sc32;
+    a.sc_f64 = p->d_sc64;
+    a.sc_ld = p->sc_ld;
+    a.bold = p->d_bold;
+    a.bold_f64 = p->d_bold64;
+    a.wIE_out = p->d_wIE_out;
+    a.trials = p->d_trials;
+    a.failed = p->d_failed;
+    a.ext = p->d_ext;
+    a.work_counter = p->d_counter;
+    a.status = p->d_status;
+    return a;
+}
+
 extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_ee, const double* w_ei,
                        const double* w_ie, bnm_batch_out* out) {
     if (!p || !out || !G || !w_ee || !w_ei) return fail(BNM_EINVAL, "null argument");
@@ -733,35 +782,7 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_hist, 0, (size_t)n * (p->m + 1) * 4, st));
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_eq, 0, (size_t)n * (p->m + 1) * 4, st));
 
-    SimArgs a;
-    std::memset(&a, 0, sizeof a);
-    a.N = N;
-    a.n_sims = n;
-    a.T = c.time_steps;
-    a.TR = c.bold_tr;
-    a.frames = s.frames;
-    a.n_vols_remove = s.n_vols_remove;
-    a.adjust_fic = c.do_fic && c.numerical_fic;
-    a.max_trials = c.max_fic_trials;
-    a.samp_start = c.i_sampling_start;
-    a.samp_end = c.i_sampling_end;
-    a.init_delta = c.init_delta;
-    a.G = p->d_G;
-    a.wEE = p->d_wEE;
-    a.wEI = p->d_wEI;
-    a.wIE = p->d_wIE;
-    a.noise = p->d_noise;
-    a.sc_f32 = p->d_sc32;
-    a.sc_f64 = p->d_sc64;
-    a.sc_ld = p->sc_ld;
-    a.bold = p->d_bold;
-    a.bold_f64 = p->d_bold64;
-    a.wIE_out = p->d_wIE_out;
-    a.trials = p->d_trials;
-    a.failed = p->d_failed;
-    a.ext = p->d_ext;
-    a.work_counter = p->d_counter;
-    a.status = p->d_status;
+    const SimArgs a = sim_args(p, n);
     if (c.precision == BNM_PREC_F32) {
         if ((rc = tune_integrator(p, a))) return rc;
         BNM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, 16, st));
@@ -813,6 +834,281 @@ extern "C" int bnm_check_fit_bold(bnm_plan* p, int32_t n, const double* bold, bn
     int rc = launch_analysis(p, n, 0);
     if (rc) return rc;
     return finish(p, n, out, false);
+}
+
+
+// ------------------------------------------------------------ groups
+//
+// Several plans (subjects of different node counts) run as one CUDA graph per
+// call: each plan's stages on its own stream, forked from and joined to an
+// origin stream, with inputs and outputs staged through pinned host buffers
+// so the whole generation is one graph launch and one host synchronisation.
+
+static int ensure_pinned(bnm_plan* p) {
+    if (p->pinned) return BNM_OK;
+    const size_t n = p->cfg.max_sims, N = p->cfg.nodes;
+    const size_t doubles = n * 3 * N + n * 5 + n * N, ints = n * 3 + 4;
+    BNM_CUDA_TRY(cudaMallocHost((void**)&p->pinned, doubles * 8 + ints * 4));
+    double* d = reinterpret_cast<double*>(p->pinned);
+    p->io_G = d;
+    p->io_wEE = p->io_G + n;
+    p->io_wEI = p->io_wEE + n * N;
+    p->io_cost = p->io_wEI + n * N;
+    p->io_pen = p->io_cost + n;
+    p->io_fcc = p->io_pen + n;
+    p->io_fcdiff = p->io_fcc + n;
+    p->io_ks = p->io_fcdiff + n;
+    p->io_wie = p->io_ks + n;
+    int* q = reinterpret_cast<int*>(p->io_wie + n * N);
+    p->io_failed = q;
+    p->io_trials = q + n;
+    p->io_unstable = q + 2 * n;
+    p->io_status = q + 3 * n;
+    return BNM_OK;
+}
+
+// One generation of a plan from its pinned inputs to its pinned outputs,
+// stream operations only (capturable).  The integrator must be tuned.
+static int enqueue_run(bnm_plan* p, int n) {
+    const bnm_config& c = p->cfg;
+    const bnm_sizes& s = p->sz;
+    const int N = c.nodes;
+    cudaStream_t st = p->st;
+    int rc;
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->d_G, p->io_G, n * 8, cudaMemcpyHostToDevice, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->d_wEE, p->io_wEE, (size_t)n * N * 8, cudaMemcpyHostToDevice, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->d_wEI, p->io_wEI, (size_t)n * N * 8, cudaMemcpyHostToDevice, st));
+    BNM_CUDA_TRY(rec(p, p->ev[0]));
+    p->launches = 2;
+    if ((rc = launch_fic(p, n))) return rc;
+    BNM_CUDA_TRY(rec(p, p->ev[1]));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, 16, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_nan, 0, n * 4, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_wsum, 0, (size_t)n * std::max(s.n_windows, 1) * 2 * 8, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_hist, 0, (size_t)n * (p->m + 1) * 4, st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_eq, 0, (size_t)n * (p->m + 1) * 4, st));
+    const SimArgs a = sim_args(p, n);
+    if (c.precision == BNM_PREC_F32)
+        BNM_CUDA_TRY(bnm_launch_integrate_shape(a, p->shape, p->num_sms, st));
+    else
+        BNM_CUDA_TRY(bnm_launch_integrate_exact(a, c.precision == BNM_PREC_F64, p->num_sms, st));
+    BNM_CUDA_TRY(rec(p, p->ev[2]));
+    if ((rc = launch_analysis(p, n, c.calculate_fic_penalty))) return rc;
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_status, p->d_status, 4, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_cost, p->d_cost, n * 8, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_pen, p->d_pen, n * 8, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_fcc, p->d_fcc, n * 8, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_fcdiff, p->d_fcdiff, n * 8, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_ks, p->d_ks, n * 8, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_wie, p->d_wIE_out, (size_t)n * N * 8, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_failed, p->d_failed, n * 4, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_trials, p->d_trials, n * 4, cudaMemcpyDeviceToHost, st));
+    BNM_CUDA_TRY(cudaMemcpyAsync(p->io_unstable, p->d_unstable, n * 4, cudaMemcpyDeviceToHost, st));
+    return BNM_OK;
+}
+
+// Stage timings of a finished enqueued run (the events ran on the device).
+static int read_timings(bnm_plan* p) {
+    float ms;
+    for (int i = 0; i < 5; i++) {
+        BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->ev[i], p->ev[i + 1]));
+        p->timings[i] = ms;
+    }
+    BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->ev[0], p->ev[5]));
+    p->timings[5] = ms;
+    p->gram_ms[0] = p->gram_ms[1] = 0;
+    for (int g = 0; g < p->n_gram; g++) {
+        BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->gev[2 * g], p->gev[2 * g + 1]));
+        p->gram_ms[g == 0 ? 0 : 1] += ms;
+    }
+    return BNM_OK;
+}
+
+struct bnm_group {
+    std::vector<bnm_plan*> plans;
+    std::vector<int> n;  // batch sizes the graph was captured for
+    cudaStream_t origin = nullptr;
+    cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    double last_ms = 0;
+    int graph_launched = 0;
+};
+
+extern "C" void bnm_group_destroy(bnm_group* g) {
+    if (!g) return;
+    if (!g->plans.empty()) cudaSetDevice(g->plans[0]->cfg.device);
+    if (g->origin) cudaStreamSynchronize(g->origin);
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    for (cudaEvent_t e : g->join)
+        if (e) cudaEventDestroy(e);
+    for (cudaEvent_t e : {g->fork, g->t0, g->t1})
+        if (e) cudaEventDestroy(e);
+    if (g->origin) cudaStreamDestroy(g->origin);
+    delete g;
+}
+
+static int group_create(bnm_plan* const* plans, int n_plans, bnm_group* g) {
+    for (int i = 0; i < n_plans; i++) {
+        if (!plans[i]) return fail(BNM_EINVAL, "plan %d is null", i);
+        if (plans[i]->cfg.device != plans[0]->cfg.device) return fail(BNM_EINVAL, "plans of a group share one device");
+        if (!plans[i]->cfg.do_fic) return fail(BNM_EINVAL, "group runs use device FIC: plan %d has do_fic = 0", i);
+        for (int j = 0; j < i; j++)
+            if (plans[j] == plans[i]) return fail(BNM_EINVAL, "plan %d appears twice", i);
+        g->plans.push_back(plans[i]);
+    }
+    BNM_CUDA_TRY(cudaSetDevice(plans[0]->cfg.device));
+    BNM_CUDA_TRY(cudaStreamCreateWithFlags(&g->origin, cudaStreamNonBlocking));
+    BNM_CUDA_TRY(cudaEventCreateWithFlags(&g->fork, cudaEventDisableTiming));
+    BNM_CUDA_TRY(cudaEventCreate(&g->t0));
+    BNM_CUDA_TRY(cudaEventCreate(&g->t1));
+    g->join.assign(n_plans, nullptr);
+    for (auto& e : g->join) BNM_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    for (bnm_plan* p : g->plans) {
+        int rc = ensure_pinned(p);
+        if (rc) return rc;
+    }
+    return BNM_OK;
+}
+
+extern "C" int bnm_group_create(bnm_plan* const* plans, int32_t n_plans, bnm_group** out) {
+    if (!plans || !out || n_plans < 1) return fail(BNM_EINVAL, "null argument or empty group");
+    *out = nullptr;
+    bnm_group* g = new bnm_group();
+    int rc = group_create(plans, n_plans, g);
+    if (rc) {
+        bnm_group_destroy(g);
+        return rc;
+    }
+    *out = g;
+    return BNM_OK;
+}
+
+static int capture(bnm_group* g) {
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    g->exec = nullptr;
+    g->graph = nullptr;
+    BNM_CUDA_TRY(cudaStreamBeginCapture(g->origin, cudaStreamCaptureModeRelaxed));
+    int rc = BNM_OK;
+    cudaError_t e = cudaEventRecord(g->fork, g->origin);
+    for (size_t i = 0; i < g->plans.size() && e == cudaSuccess && !rc; i++) {
+        bnm_plan* p = g->plans[i];
+        e = cudaStreamWaitEvent(p->st, g->fork, 0);
+        if (e != cudaSuccess) break;
+        p->capturing = true;
+        rc = enqueue_run(p, g->n[i]);
+        p->capturing = false;
+        if (!rc) e = cudaEventRecord(g->join[i], p->st);
+        if (!rc && e == cudaSuccess) e = cudaStreamWaitEvent(g->origin, g->join[i], 0);
+    }
+    cudaGraph_t graph = nullptr;
+    const cudaError_t e_end = cudaStreamEndCapture(g->origin, &graph);
+    if (rc) {
+        if (graph) cudaGraphDestroy(graph);
+        return rc;
+    }
+    BNM_CUDA_TRY(e);
+    BNM_CUDA_TRY(e_end);
+    g->graph = graph;
+    BNM_CUDA_TRY(cudaGraphInstantiate(&g->exec, g->graph, 0));
+    return BNM_OK;
+}
+
+extern "C" int bnm_group_run(bnm_group* g, const int32_t* n, const double* const* G, const double* const* w_ee,
+                             const double* const* w_ei, bnm_batch_out* outs) {
+    if (!g || !n || !G || !w_ee || !w_ei || !outs) return fail(BNM_EINVAL, "null argument");
+    const size_t np = g->plans.size();
+    BNM_CUDA_TRY(cudaSetDevice(g->plans[0]->cfg.device));
+    std::vector<int> sizes(np);
+    for (size_t i = 0; i < np; i++) {
+        bnm_plan* p = g->plans[i];
+        const int N = p->cfg.nodes;
+        if (n[i] < 1 || n[i] > p->cfg.max_sims) return fail(BNM_EINVAL, "plan %zu: n=%d outside [1, max_sims]", i, n[i]);
+        if (!G[i] || !w_ee[i] || !w_ei[i]) return fail(BNM_EINVAL, "plan %zu: null parameters", i);
+        const bool rf = p->cfg.precision == BNM_PREC_F32_REF;
+        for (int k = 0; k < n[i]; k++) {
+            if (!std::isfinite(G[i][k])) return fail(BNM_EINVAL, "plan %zu: G[%d] is not finite", i, k);
+            p->io_G[k] = rf ? (double)(float)G[i][k] : G[i][k];
+        }
+        for (size_t k = 0; k < (size_t)n[i] * N; k++) {
+            if (!std::isfinite(w_ee[i][k]) || !std::isfinite(w_ei[i][k]))
+                return fail(BNM_EINVAL, "plan %zu: wEE/wEI not finite at %zu", i, k);
+            p->io_wEE[k] = rf ? (double)(float)w_ee[i][k] : w_ee[i][k];
+            p->io_wEI[k] = rf ? (double)(float)w_ei[i][k] : w_ei[i][k];
+        }
+        sizes[i] = n[i];
+    }
+    int rc;
+    if (!g->exec || sizes != g->n) {
+        // first call for these batch sizes: run eagerly (this tunes every
+        // plan's integrator, which a capture cannot do), then capture the graph
+        g->n = sizes;
+        for (size_t i = 0; i < np; i++) {
+            bnm_plan* p = g->plans[i];
+            if (p->cfg.precision == BNM_PREC_F32) {
+                BNM_CUDA_TRY(cudaMemcpy(p->d_G, p->io_G, sizes[i] * 8, cudaMemcpyHostToDevice));
+                BNM_CUDA_TRY(cudaMemcpy(p->d_wEE, p->io_wEE, (size_t)sizes[i] * p->cfg.nodes * 8, cudaMemcpyHostToDevice));
+                BNM_CUDA_TRY(cudaMemcpy(p->d_wEI, p->io_wEI, (size_t)sizes[i] * p->cfg.nodes * 8, cudaMemcpyHostToDevice));
+                if ((rc = launch_fic(p, sizes[i]))) return rc;
+                if ((rc = tune_integrator(p, sim_args(p, sizes[i])))) return rc;
+            }
+        }
+        BNM_CUDA_TRY(cudaEventRecord(g->t0, g->origin));
+        BNM_CUDA_TRY(cudaEventRecord(g->fork, g->origin));
+        for (size_t i = 0; i < np; i++) {
+            bnm_plan* p = g->plans[i];
+            BNM_CUDA_TRY(cudaStreamWaitEvent(p->st, g->fork, 0));
+            if ((rc = enqueue_run(p, sizes[i]))) return rc;
+            BNM_CUDA_TRY(cudaEventRecord(g->join[i], p->st));
+            BNM_CUDA_TRY(cudaStreamWaitEvent(g->origin, g->join[i], 0));
+        }
+        BNM_CUDA_TRY(cudaEventRecord(g->t1, g->origin));
+        BNM_CUDA_TRY(cudaStreamSynchronize(g->origin));
+        g->graph_launched = 0;
+        if ((rc = capture(g))) return rc;
+    } else {
+        BNM_CUDA_TRY(cudaEventRecord(g->t0, g->origin));
+        BNM_CUDA_TRY(cudaGraphLaunch(g->exec, g->origin));
+        BNM_CUDA_TRY(cudaEventRecord(g->t1, g->origin));
+        BNM_CUDA_TRY(cudaStreamSynchronize(g->origin));
+        g->graph_launched = 1;
+    }
+    float ms;
+    BNM_CUDA_TRY(cudaEventElapsedTime(&ms, g->t0, g->t1));
+    g->last_ms = ms;
+    for (size_t i = 0; i < np; i++) {
+        bnm_plan* p = g->plans[i];
+        const int k = sizes[i], N = p->cfg.nodes;
+        if ((rc = read_timings(p))) return rc;
+        const int status = *p->io_status;
+        if (status & kStatusTimeout) return fail(BNM_ETIMEOUT, "plan %zu: a device wait gave up (status %d)", i, status);
+        if (status) return fail(BNM_ECUDA, "plan %zu: device status %d", i, status);
+        bnm_batch_out& o = outs[i];
+        auto put = [](auto* dst, const auto* src, size_t cnt) {
+            if (dst) std::copy(src, src + cnt, dst);
+        };
+        put(o.cost, p->io_cost, k);
+        put(o.fic_penalty, p->io_pen, k);
+        put(o.fc_corr, p->io_fcc, k);
+        put(o.fc_diff, p->io_fcdiff, k);
+        put(o.fcd_ks, p->io_ks, k);
+        put(o.w_ie, p->io_wie, (size_t)k * N);
+        put(o.fic_failed, p->io_failed, k);
+        put(o.fic_ntrials, p->io_trials, k);
+        put(o.fic_unstable, p->io_unstable, k);
+    }
+    return BNM_OK;
+}
+
+extern "C" int bnm_group_last(bnm_group* g, double* ms, int32_t* graph_launched) {
+    if (!g || !ms) return fail(BNM_EINVAL, "null argument");
+    *ms = g->last_ms;
+    if (graph_launched) *graph_launched = g->graph_launched;
+    return BNM_OK;
 }
 
 extern "C" int bnm_last_gram(bnm_plan* p, double* ms2, int32_t* launches) {

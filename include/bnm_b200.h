@@ -148,6 +148,27 @@ int bnm_analytic_fic(bnm_plan *plan, int32_t n, const double *G, const double *w
 
 /* Time of the last bnm_run on the device, per stage, in ms:
  * [0] analytic FIC, [1] integration, [2] FC + window FC, [3] FCD + KS histogram, [4] GOF, [5] total. */
+/* Groups: several plans (e.g. subjects of different node counts, each with
+ * its own SC, targets and autotuned integrator) run one generation as one
+ * CUDA graph launch: every plan's stages on its own stream, forked from and
+ * joined to one origin stream, parameters and results staged through pinned
+ * host buffers, one host synchronisation.  No counterpart in the reference,
+ * which runs one subject per process.  The first bnm_group_run for a set of
+ * batch sizes runs eagerly (and tunes each plan's integrator) and captures
+ * the graph; later calls with the same sizes launch it.  Plans must use
+ * device FIC (do_fic = 1); outputs per plan: cost, fic_penalty, fc_corr,
+ * fc_diff, fcd_ks, w_ie, fic_failed, fic_ntrials, fic_unstable (bold, fc,
+ * fcd and ext_means are not filled). */
+typedef struct bnm_group bnm_group;
+int bnm_group_create(bnm_plan *const *plans, int32_t n_plans, bnm_group **out);
+void bnm_group_destroy(bnm_group *group);
+int bnm_group_run(bnm_group *group, const int32_t *n, const double *const *G, const double *const *w_ee,
+                  const double *const *w_ei, bnm_batch_out *outs);
+/* Device time of the last group run (ms, events on the origin stream around
+ * the whole generation) and whether it was a graph launch (1) or the eager
+ * first run (0). */
+int bnm_group_last(bnm_group *group, double *ms, int32_t *graph_launched);
+
 /* Device time of the tensor-core Gram kernels alone in the last bnm_run /
  * bnm_check_fit_bold (ms2[0]: FC Gram, ms2[1]: FCD Gram summed over staged
  * chunks; 0 with BNM_GRAM_F32) and the number of library kernels that call

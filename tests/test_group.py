@@ -1,0 +1,76 @@
+"""Groups (bnm_group_*): subjects of different node counts, each with its own
+SC, targets and autotuned integrator, run one generation as one CUDA graph.
+The eager first call, and the graph launches after it, must give the same
+results as each plan's own bnm_run on the same inputs."""
+import numpy as np
+import pytest
+
+import bnm_cuda_b200 as B
+from bnm_cuda_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+NODES = (16, 48, 160)  # register kernel, register kernel, cluster kernel
+
+
+def _subjects(n):
+    plans, params = [], []
+    for k, N in enumerate(NODES):
+        sc = synth.make_sc(N, 0.3, 10 + k)
+        cfg = B.Config(nodes=N, max_sims=8, time_steps=12000, bold_tr=500, window_size=10, window_step=2,
+                       bold_remove_s=2)
+        s = cfg.sizes()
+        rng = np.random.default_rng(k)
+        plans.append(B.Plan(cfg, sc, rng.uniform(-0.2, 0.8, s["n_pairs"]), rng.uniform(-0.3, 1.0, 300)))
+        params.append(synth.uniform_params(n, N, 30 + k))
+    return plans, params
+
+
+def _same(a, b):
+    np.testing.assert_array_equal(a["fic_ntrials"], b["fic_ntrials"])
+    np.testing.assert_array_equal(a["fic_failed"], b["fic_failed"])
+    for k in ("cost", "fic_penalty", "fc_corr", "fc_diff", "fcd_ks"):
+        np.testing.assert_allclose(a[k], b[k], rtol=0, atol=1e-9, err_msg=k)
+    np.testing.assert_allclose(a["w_ie"], b["w_ie"], rtol=0, atol=1e-9)
+
+
+def test_group_graph_matches_per_plan_runs():
+    plans, params = _subjects(5)
+    solo = [p.run(*prm, outputs=("w_ie",)) for p, prm in zip(plans, params)]
+    with B.Group(plans) as g:
+        first = g.run(params)
+        assert not g.last()["graph"]
+        second = g.run(params)
+        assert g.last()["graph"] and g.last()["ms"] > 0
+        for a, b, c in zip(solo, first, second):
+            _same(a, b)
+            _same(a, c)
+        # new parameters, same batch sizes: the graph is reused
+        params2 = [synth.uniform_params(5, p.cfg.nodes, 99 + k) for k, p in enumerate(plans)]
+        third = g.run(params2)
+        assert g.last()["graph"]
+    for p, prm, r in zip(plans, params2, third):
+        _same(p.run(*prm, outputs=("w_ie",)), r)
+    kinds = [p.integrator()["kind"] for p in plans]
+    assert kinds == ["register", "register", "cluster"], kinds
+    for p in plans:
+        p.close()
+
+
+def test_group_rejects_bad_inputs():
+    plans, params = _subjects(3)
+    with B.Group(plans) as g:
+        bad = list(params)
+        G = bad[1][0].copy()
+        G[0] = np.inf
+        bad[1] = (G, bad[1][1], bad[1][2])
+        with pytest.raises(B.BnmError) as e:
+            g.run(bad)
+        assert e.value.code == B.BNM_EINVAL
+        with pytest.raises(B.BnmError):
+            g.run([(np.ones(9), 0.2, 0.2)] + params[1:])  # more than max_sims
+        g.run(params)  # still usable
+    with pytest.raises(B.BnmError):
+        B.Group([plans[0], plans[0]])
+    for p in plans:
+        p.close()
