@@ -460,6 +460,77 @@ def run_precision(args):
     return 0
 
 
+def run_subjects(args):
+    """Uneven-size batching: 8 subjects with N = 68, 68, 100, 100, 200, 200,
+    400, 400 (own seeded SC each, 30 % density, seeds 0..7), 64 CMA-ES
+    particles per subject (512 simulations per generation), 300 s at TR 1 s,
+    window 44 step 1, 30 s removed, FIC on.  Every generation is one CUDA graph
+    launch over all subjects (bnm_group_run), each subject's integrator picked
+    by the autotuner for its N (register kernel and particles per CTA for
+    N <= 128, cluster size / nodes per warp / SC chunks in registers above).
+    The first generation runs eagerly (tuning, graph capture) and is reported
+    apart; sims/s is over the --subject-generations - 1 graph launches after it."""
+    import bnm_cuda_b200 as B
+    from bnm_cuda_b200 import synth
+    from bnm_cuda_b200.surrogate import Bounds
+
+    nodes, lam, T = [68, 68, 100, 100, 200, 200, 400, 400], 64, 300_000
+    gens = max(2, args.subject_generations)
+    bounds = Bounds()
+    plans, cms = [], []
+    for k, N in enumerate(nodes):
+        sc = synth.make_sc(N, 0.3, k)
+        cfg = B.Config(nodes=N, max_sims=lam, time_steps=T, bold_tr=1000, window_size=WS, window_step=1,
+                       bold_remove_s=REMOVE_S, noise_seed=410)
+        s = cfg.sizes()
+        tcfg = B.Config(**{**cfg.__dict__, "max_sims": 1, "noise_seed": 1})
+        with B.Plan(tcfg, sc, np.zeros(s["n_pairs"]), np.zeros(s["n_fcd"])) as tp:
+            tr = tp.run(2.0, 0.3, 0.2, outputs=("fc", "fcd"))
+        plans.append(B.Plan(cfg, sc, tr["fc"][0], tr["fcd"][0]))
+        cms.append(B.CMAES(lam, 3, 1 + k, gens + 1, from_env=False))
+    gen_ms, walls, graph, best, trials = [], [], [], [np.inf] * len(nodes), []
+    with ClockSampler(0) as clk, B.Group(plans) as g:
+        for gen in range(gens):
+            params = []
+            for es, N in zip(cms, nodes):
+                feas, _, _ = es.samples()
+                Gv, we, wi = bounds.to_params(feas)
+                params.append((Gv, np.repeat(we[:, None], N, 1), np.repeat(wi[:, None], N, 1)))
+            t0 = time.perf_counter()
+            res = g.run(params)
+            walls.append(time.perf_counter() - t0)
+            last = g.last()
+            gen_ms.append(last["ms"])
+            graph.append(last["graph"])
+            trials.append([float(r["fic_ntrials"].mean()) for r in res])
+            for k, (es, r) in enumerate(zip(cms, res)):
+                cost = r["cost"] + r["fic_penalty"]
+                best[k] = min(best[k], float(cost.min()))
+                es.tell(cost)
+        shapes = [p.integrator() for p in plans]
+        launches = sum(p.gram_timing()["launches"] for p in plans)
+    timed_ms, timed_wall = float(np.sum(gen_ms[1:])), float(np.sum(walls[1:]))
+    n_timed = len(gen_ms) - 1
+    print(json.dumps({
+        "metric": "sims/s", "value": 512 * n_timed / (timed_ms / 1e3), "unit": "sims/s", "n_gpus": 1,
+        "steps": n_timed, "warmup": 1, "ms_per_step": timed_ms / n_timed, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "uneven-subjects-N68-100-200-400x2-300s-lambda64", "nodes": nodes, "particles": lam,
+                   "model_time_ms": T, "tr_ms": 1000, "window": WS, "step": 1, "generations": gens,
+                   "integrators": [{"nodes": N, **sh} for N, sh in zip(nodes, shapes)],
+                   "graph": "one CUDA graph launch per generation over 8 subject streams"},
+        "e2e": {"value": 512 * n_timed / timed_wall, "unit": "sims/s",
+                "h2d_bytes_per_step": sum(8 * (lam + 2 * lam * N) for N in nodes),
+                "d2h_bytes_per_step": sum(8 * lam * (5 + N) + 12 * lam for N in nodes)},
+        "gpu_launches": launches * n_timed,
+        "generation_ms": gen_ms, "graph_launched": graph, "first_generation_eager_ms": gen_ms[0],
+        "mean_fic_trials": trials[-1], "best_cost": best, "clocks": clk.summary(),
+    }))
+    for p in plans:
+        p.close()
+    return 0
+
+
 def main():
     global N_SIMS, T_MS, WORKLOAD
     ap = argparse.ArgumentParser()
@@ -467,9 +538,11 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="generation", choices=["generation", "surrogate", "precision"],
+    ap.add_argument("--workload", default="generation", choices=["generation", "surrogate", "precision", "subjects"],
                     help="generation: one CMA-ES generation (headline); surrogate: screened vs plain CMA-ES; "
-                         "precision: FC/FCD Gram arithmetic against FP64 at N=400")
+                         "precision: FC/FCD Gram arithmetic against FP64 at N=400; subjects: 8 subjects of "
+                         "N = 68..400 in one graph per generation")
+    ap.add_argument("--subject-generations", type=int, default=4, help="subjects: generations (first is eager)")
     ap.add_argument("--check-sims", type=int, default=4, help="precision: particles checked against FP64")
     ap.add_argument("--gram", default="bf16x3", choices=["f32", "bf16", "bf16x3"],
                     help="generation: FC/FCD Gram arithmetic")
@@ -489,6 +562,8 @@ def main():
         return run_surrogate(args)
     if args.workload == "precision":
         return run_precision(args)
+    if args.workload == "subjects":
+        return run_subjects(args)
     return run_b200(args)
 
 

@@ -465,6 +465,11 @@ static int tune_integrator(bnm_plan* p, const SimArgs& a) {
         }
         cudaGetLastError();  // a shape that cannot launch is skipped
         BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
+        int st_word = 0;
+        BNM_CUDA_TRY(cudaMemcpy(&st_word, p->d_status, 4, cudaMemcpyDeviceToHost));
+        if (st_word)
+            return fail(BNM_ETIMEOUT, "integrator tuning: shape %d,%d,%d,%d,%d for N=%d n=%d left status 0x%x",
+                        cand[i].kind, cand[i].slots, cand[i].csize, cand[i].rpw, cand[i].kr, a.N, n, st_word);
         if (!ok) continue;
         BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->tev[0], p->tev[1]));
         p->n_tried++;
