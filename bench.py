@@ -49,11 +49,13 @@ SAMPLE_MS = 12_000
 WORKLOAD = "cmaes-generation-N100-450s-x256"
 
 
-def workload_inputs(rank: int = 0):
+def workload_inputs(world: int = 1):
+    """SC and the whole population: N_SIMS particles per rank (weak scaling);
+    rank r simulates particles [r N_SIMS, (r+1) N_SIMS) (bnm_cuda_b200.shard)."""
     from bnm_cuda_b200 import synth
 
     sc = synth.make_sc(N_NODES, 0.3, 0)
-    G, wEE, wEI = synth.uniform_params(N_SIMS, N_NODES, 1 + rank)
+    G, wEE, wEI = synth.uniform_params(N_SIMS * world, N_NODES, 1)
     return sc, G, wEE, wEI
 
 
@@ -230,7 +232,11 @@ def run_b200(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
 
-    sc, G, wEE, wEI = workload_inputs(rank)
+    from bnm_cuda_b200 import shard
+
+    sc, G_all, wEE_all, wEI_all = workload_inputs(world)
+    a, b = shard.shard_bounds(len(G_all), world, rank)
+    G, wEE, wEI = G_all[a:b], wEE_all[a:b], wEI_all[a:b]
     emp_fc, emp_fcd = make_targets(sc)
     gram = {"f32": B.GRAM_F32, "bf16": B.GRAM_BF16, "bf16x3": B.GRAM_BF16_SPLIT}[args.gram]
     cfg = B.Config(nodes=N_NODES, max_sims=N_SIMS, time_steps=T_MS, bold_tr=TR, window_size=WS, window_step=STEP,
@@ -251,19 +257,18 @@ def run_b200(args):
     with ClockSampler(local) as clk:
         for _ in range(args.steps):
             t0 = time.perf_counter()
-            r = plan.run(G, wEE, wEI, outputs=outputs)
-            if dist:
-                import torch
-                c = torch.tensor(r["cost"], device=f"cuda:{local}")
-                gathered = [torch.empty_like(c) for _ in range(world)]
-                dist.all_gather(gathered, c)
+            if dist:  # this rank's shard, then every particle's fit terms on every rank (NCCL)
+                r = shard.run_sharded(lambda g, e, i: plan.run(g, e, i, outputs=outputs), G_all, wEE_all, wEI_all)
                 torch.cuda.synchronize()
+            else:
+                r = plan.run(G, wEE, wEI, outputs=outputs)
             wall.append(time.perf_counter() - t0)
             t = plan.timings()
             launches += plan.gram_timing()["launches"]
             dev_ms.append(t["total"])
             integ_ms.append(t["integrate"])
-            subs = 10 * (T_MS + 1) + 100_000 * r["fic_ntrials"].astype(np.float64)
+            subs = 10 * (T_MS + 1) + 100_000 * np.asarray(r["fic_ntrials"], np.float64)[a:b] if dist else \
+                10 * (T_MS + 1) + 100_000 * r["fic_ntrials"].astype(np.float64)
             flops.append(2.0 * N_NODES * N_NODES * subs.sum())
     barrier()
     dev_total, wall_total = float(np.sum(dev_ms)) / 1e3, float(np.sum(wall))
