@@ -145,7 +145,7 @@ def cpu_reference_sample(n_threads: int, sample_ms: int = SAMPLE_MS):
 
     if not ref.ref_available():
         return None
-    sc, G, wEE, wEI = workload_inputs(0)
+    sc, G, wEE, wEI = workload_inputs(1)
     idx = np.arange(n_threads) % N_SIMS
     n = len(idx)
     zeros = np.zeros((n, N_NODES))
