@@ -244,7 +244,10 @@ __global__ void __launch_bounds__(256) fcd_gram_kernel(FcdArgs a) {
                 if (a.fcd) a.fcd[(size_t)sim * a.n_fcd + idx] = v;
                 int c;
                 bool equal;
-                ks_bucket(a.emp_sorted, a.m, (double)v, c, equal);
+                if (a.ks_lut)
+                    ks_bucket_lut(a.emp_sorted, a.ks_lut, a.m, (double)v, c, equal);
+                else
+                    ks_bucket(a.emp_sorted, a.m, (double)v, c, equal);
                 atomicAdd(&hist[c], 1u);
                 if (equal) atomicAdd(&eq[c], 1u);
             }

@@ -141,6 +141,7 @@ struct bnm_plan {
     float* d_noise = nullptr;
     int *d_pi = nullptr, *d_pj = nullptr;
     double *d_emp_fc = nullptr, *d_emp_sorted = nullptr;
+    int* d_ks_lut = nullptr;
     unsigned char* d_valid = nullptr;
     double *d_G = nullptr, *d_wEE = nullptr, *d_wEI = nullptr, *d_wIE = nullptr, *d_wIE_out = nullptr;
     int* d_unstable = nullptr;
@@ -284,6 +285,12 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
     BNM_CUDA_TRY(dalloc(p, &p->d_emp_sorted, es.size()));
     BNM_CUDA_TRY(dalloc(p, &p->d_valid, valid.size()));
     BNM_CUDA_TRY(cudaMemcpy(p->d_emp_sorted, es.data(), es.size() * 8, cudaMemcpyHostToDevice));
+    std::vector<int> lut(kKsBuckets + 1, 0);
+    for (int b = 1; b < kKsBuckets; b++)
+        lut[b] = (int)(std::lower_bound(es.begin(), es.end(), ks_edge(b)) - es.begin());
+    lut[kKsBuckets] = p->m;
+    BNM_CUDA_TRY(dalloc(p, &p->d_ks_lut, lut.size()));
+    BNM_CUDA_TRY(cudaMemcpy(p->d_ks_lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice));
     BNM_CUDA_TRY(cudaMemcpy(p->d_valid, valid.data(), valid.size(), cudaMemcpyHostToDevice));
 
     // per-particle work space
@@ -608,6 +615,7 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
             ga.out = p->d_fcd + (size_t)c0 * s.n_fcd;
             ga.out_ld = s.n_fcd;
             ga.emp_sorted = p->d_emp_sorted;
+            ga.ks_lut = p->d_ks_lut;
             ga.m = p->m;
             ga.hist = p->d_hist + (size_t)c0 * (p->m + 1);
             ga.eq = p->d_eq + (size_t)c0 * (p->m + 1);
@@ -629,6 +637,7 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
         da.fcd = p->d_fcd;
         da.n_fcd = s.n_fcd;
         da.emp_sorted = p->d_emp_sorted;
+        da.ks_lut = p->d_ks_lut;
         da.m = p->m;
         da.hist = p->d_hist;
         da.eq = p->d_eq;

@@ -337,7 +337,10 @@ __global__ void __launch_bounds__(192, 1) gram_tc_kernel(GramArgs a) {
             if (hist) {
                 int c;
                 bool equal;
-                ks_bucket(a.emp_sorted, a.m, (double)x, c, equal);
+                if (a.ks_lut)
+                    ks_bucket_lut(a.emp_sorted, a.ks_lut, a.m, (double)x, c, equal);
+                else
+                    ks_bucket(a.emp_sorted, a.m, (double)x, c, equal);
                 atomicAdd(&hist[c], 1u);
                 if (equal) atomicAdd(&eq[c], 1u);
             }

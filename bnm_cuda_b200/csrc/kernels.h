@@ -31,6 +31,7 @@ struct FcdArgs {
     int m;
     unsigned int* hist;     // [n][m+1] counts by upper_bound rank
     unsigned int* eq;       // [n][m+1] sim values equal to emp_sorted[c-1]
+    const int* ks_lut;      // bucket table of emp_sorted (kKsBuckets + 1), or null
     int* nan_flag;
     int tiles;              // tiles per side
 };
@@ -74,6 +75,30 @@ __device__ __forceinline__ void ks_bucket(const double* e, int m, double x, int&
     equal = (c > 0) && (e[c - 1] == x);
 }
 
+// Bucket table over the sorted empirical FCD for the KS rank search: bucket b
+// covers [edge(b), edge(b+1)) with edge(b) = -1 + b 2^-15 (exact in double),
+// bucket 0 extends to -inf and the last to +inf; lut[b] = #emp < edge(b)
+// (lut[0] = 0, lut[kKsBuckets] = m).  A correlation's rank is then found by
+// two table loads and an upper_bound over the few values of its bucket.
+constexpr int kKsBuckets = 1 << 16;
+__host__ __device__ __forceinline__ double ks_edge(int b) { return -1.0 + b * (1.0 / 32768.0); }
+
+__device__ __forceinline__ void ks_bucket_lut(const double* e, const int* lut, int m, double x, int& c, bool& equal) {
+    const double t = (x + 1.0) * 32768.0;
+    int b = t < 1.0 ? 0 : (t >= (double)(kKsBuckets - 1) ? kKsBuckets - 1 : (int)t);
+    // x + 1 can round across an edge when |x| is tiny: settle b on the exact edges
+    if (b > 0 && x < ks_edge(b)) b--;
+    if (b < kKsBuckets - 1 && x >= ks_edge(b + 1)) b++;
+    int lo = lut[b], hi = lut[b + 1];
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (e[mid] <= x) lo = mid + 1; else hi = mid;
+    }
+    c = lo;
+    equal = (c > 0) && (e[c - 1] == x);
+    (void)m;
+}
+
 // Tensor-core Gram operands: rows x K values as BF16 tiles of 128 rows x 64 K
 // (16 KB, the tcgen05 K-major SWIZZLE_128B layout), tile (sim, row block,
 // k block) at ((sim * row_blocks + rb) * kblocks + kb) * 16384 bytes.
@@ -101,6 +126,7 @@ struct GramArgs {
     int m;
     unsigned int* hist;
     unsigned int* eq;
+    const int* ks_lut;        // bucket table (see ks_bucket_lut), or null
     int* nan_flag;            // [n]
     int* status;
 };

@@ -187,7 +187,7 @@ extern "C" int bnm_gof_noalloc(const float* d_bold, int32_t n, int32_t frames, i
     BNM_CUDA_TRY(bnm_launch_fc_window(fa, st));
 
     FcdArgs da;
-    std::memset(&da, 0, sizeof da);
+    std::memset(&da, 0, sizeof da);  // no bucket table: plain rank search
     da.n_sims = n;
     da.W = W;
     da.P = P;
