@@ -36,9 +36,10 @@ CU = {
     "mlp.cu": [],
     "gram_tc.cu": [],
     "integrate_cluster.cu": [],
+    "integrate_colsplit.cu": [],
 }
 CPP = ["cmaes.cpp"]
-HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h", "fp32_model.cuh"]
+HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h", "fp32_model.cuh", "cluster_util.cuh"]
 
 
 def _newer(src_paths, out):

@@ -432,8 +432,8 @@ static int upload_params(bnm_plan* p, int n, const double* G, const double* w_ee
 static int tune_integrator(bnm_plan* p, const SimArgs& a) {
     const int n = a.n_sims;
     if (p->tuned_n == n) return BNM_OK;
-    IntegratorShape cand[32];
-    const int nc = bnm_integrator_candidates(a.N, cand, 32);
+    IntegratorShape cand[128];
+    const int nc = bnm_integrator_candidates(a.N, cand, 128);
     if (nc < 1) return fail(BNM_EINVAL, "no FP32 integrator for %d nodes", a.N);
     p->shape = cand[0];
     p->n_tried = 0;

@@ -1,0 +1,444 @@
+// FP32 integrator for 128 < N <= 512, column-split layout: one
+// thread-block cluster per particle, one thread per node for the update.
+//
+// Same model, time loop, FIC restarts, BOLD and extended outputs as the
+// reference's bnm kernel (bnm.cu:72-315) and CPU path (bnm.cpp:167-290), and
+// the same arithmetic as integrate_fast.cu / integrate_cluster.cu; the
+// cluster protocol (S_E exchange by st.async on mbarriers, noise ring,
+// cluster-uniform flags) is the one of integrate_cluster.cu.  What differs is
+// the coupling mat-vec:
+//   * CTA rank c owns nodes [c R, c R + R) (R <= 32 RPL).  Warp w owns the
+//     column block [2 K2 w, 2 K2 (w+1)) of all R rows; lane l holds rows
+//     l, l + 32, ... (RPL of them) as column pairs for fma.rn.f32x2, the first
+//     KRP pairs in registers and the rest in shared memory;
+//   * every lane of a warp reads the same S_E pairs (broadcast loads), forms
+//     RPL partial row sums with no shuffles, and stores them to a [warp][row]
+//     table; after one barrier thread t < R adds the W partials of row t and
+//     updates node r0 + t alone (the row-split layout updates each node in
+//     32/RPW lanes);
+//   * two CTA barriers per substep: one after the S_E wait (all threads are
+//     past it before the buffer's next phase is armed, and the partial table
+//     of the previous substep has been read), one between partials and sums.
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+#include "kernels.h"
+#include "fp32_model.cuh"
+#include "cluster_util.cuh"
+
+namespace bnm {
+namespace {
+
+constexpr int kRing = 4;  // noise ring stages (milliseconds)
+
+// Shared-memory layout (bytes), in this order:
+//   S      [2][2 K2 W] float             S_E of every node, double buffered
+//   red    [W][32 RPL] float             per-warp partial row sums
+//   SCs    [W][RPL][K2-KRP][32] float2   shared-memory part of the SC slice
+//   ring   [kRing][10][R] float2         noise of the own nodes, per millisecond
+//   ext    [6][32 RPL] double            extended-output sums of the own nodes
+//   flags  [32] int                      late[2][8], fic[8], issue
+//   mbar   [kRing + 2] uint64            noise stages, then S_E buffers 0 and 1
+template <int RPL, int K2, int KRP>
+struct ColLayout {
+    static constexpr int kRP = 32 * RPL;
+    __host__ __device__ static size_t red_off(int W) { return (size_t)2 * W * 2 * K2 * sizeof(float); }
+    __host__ __device__ static size_t sc_off(int W) { return red_off(W) + (size_t)W * kRP * sizeof(float); }
+    __host__ __device__ static size_t ring_off(int W) {
+        return sc_off(W) + (size_t)W * RPL * (K2 - KRP) * 32 * sizeof(float2);
+    }
+    __host__ __device__ static size_t ext_off(int W, int R) { return ring_off(W) + (size_t)kRing * 10 * R * sizeof(float2); }
+    __host__ __device__ static size_t flags_off(int W, int R) { return ext_off(W, R) + (size_t)6 * kRP * sizeof(double); }
+    __host__ __device__ static size_t mbar_off(int W, int R) { return flags_off(W, R) + 32 * sizeof(int); }
+    __host__ __device__ static size_t bytes(int W, int R) { return mbar_off(W, R) + (kRing + 2) * sizeof(uint64_t); }
+};
+
+template <int RPL, int K2, int KRP>
+__global__ void integrate_colsplit_kernel(SimArgs a, int R) {
+    static_assert(RPL >= 1 && RPL <= 4, "RPL");
+    static_assert(KRP >= 0 && KRP <= K2, "KRP");
+    constexpr int KS = K2 - KRP;  // column pairs in shared memory
+    constexpr int RP = 32 * RPL;
+    typedef Model<float> C;
+    typedef ColLayout<RPL, K2, KRP> L;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    const int N = a.N;
+    const int W = blockDim.x >> 5;
+    const int NC = 2 * K2 * W;  // padded column count
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, t = threadIdx.x;
+    const uint32_t crank = cluster_rank(), csize = cluster_size();
+    const int sim = blockIdx.x / csize;
+    const int r0 = (int)crank * R;
+    const int r_own = max(0, min(N - r0, R));  // nodes this CTA updates
+    const int upd_warps = (r_own + 31) >> 5;    // warps holding node owners
+
+    float* S_buf = reinterpret_cast<float*>(smem_raw);
+    float* red = reinterpret_cast<float*>(smem_raw + L::red_off(W));
+    float2* SCs = reinterpret_cast<float2*>(smem_raw + L::sc_off(W));
+    float2* ring = reinterpret_cast<float2*>(smem_raw + L::ring_off(W));
+    double* ext = reinterpret_cast<double*>(smem_raw + L::ext_off(W, R));
+    int* flags = reinterpret_cast<int*>(smem_raw + L::flags_off(W, R));
+    uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + L::mbar_off(W, R));
+
+    const int node = r0 + t;
+    const bool act = t < r_own;  // thread t owns node r0 + t
+    const long long kSpin = 1ll << 26;
+
+    cluster_sync();  // every CTA of the cluster runs before any distributed shared memory access
+    if (t == 0) {
+        for (int b = 0; b < kRing + 2; b++)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + b)) : "memory");
+        // buffer 1 receives S_E after the first substep: N values of 4 bytes
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar + kRing + 1)),
+                     "r"(4 * N)
+                     : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int k = t; k < 2 * NC; k += blockDim.x) S_buf[k] = (k % NC) < N ? 0.001f : 0.f;
+    for (int k = t; k < 6 * RP; k += blockDim.x) ext[k] = 0.0;
+    if (t < 32) flags[t] = 0;
+
+    // SC slice: rows r0 + lane + 32 i, column pairs 2 K2 w + 2 j (+1); zero outside the matrix
+    float2 scr[RPL][KRP > 0 ? KRP : 1];
+#pragma unroll
+    for (int i = 0; i < RPL; i++) {
+        const int row = lane + 32 * i;
+#pragma unroll
+        for (int j = 0; j < K2; j++) {
+            const int col = 2 * K2 * w + 2 * j;
+            float va = 0.f, vb = 0.f;
+            if (row < r_own) {
+                const float* src = a.sc_f32 + (size_t)(r0 + row) * a.sc_ld;
+                if (col < N) va = src[col];
+                if (col + 1 < N) vb = src[col + 1];
+            }
+            if (j < KRP)
+                scr[i][j < KRP ? j : 0] = make_float2(va, vb);
+            else
+                SCs[((size_t)(w * RPL + i) * KS + (j - KRP)) * 32 + lane] = make_float2(va, vb);
+        }
+    }
+    cluster_sync();  // buffers initialised in every CTA before anyone writes remote S_E
+
+    const uint32_t s_local = smem_addr(S_buf);
+    const uint32_t flags_local = smem_addr(flags);
+    const char* noise_bytes = reinterpret_cast<const char*>(a.noise);
+    const uint32_t run_bytes = (uint32_t)(r_own * sizeof(float2));  // one substep of the own nodes
+    const double duration = (double)(a.samp_end - a.samp_start + 1);
+    const float SQ = C::sigma_model * C::sqrt_dt;
+    const float LOG2E = 1.4426950408889634f;
+    const float kDtGammaE = C::dt * C::gamma_E, kDtInvTauE = C::dt / C::tau_E;
+    const float kDtGammaI = C::dt * C::gamma_I, kDtInvTauI = C::dt / C::tau_I;
+
+    const float GJ = (float)a.G[sim] * C::J_NMDA;
+    const float wEE = act ? (float)a.wEE[(size_t)sim * N + node] : 0.f;
+    const float wEI = act ? (float)a.wEI[(size_t)sim * N + node] : 0.f;
+    float wIE = act ? (float)a.wIE[(size_t)sim * N + node] : 0.f;
+    float delta = (float)a.init_delta;
+    float S_E = 0.001f, S_I = 0.001f, IE = 0.f, II = 0.f, rE = 0.f, rI = 0.f;
+    double mean_IE = 0.0;
+    BW bw;
+    int ts = 0, frame = 0, to_frame = 1, trial = 0, ms_next = 0;
+    bool failed = false, adjusting = a.adjust_fic != 0, timed_out = false;
+    uint32_t c_cons = 0, c_issue = 0;
+    int cur = 0;
+    // S_E exchange as in integrate_cluster.cu: buffer b's mbarrier completes a
+    // phase when all N values of the next S_E have landed; ph bit b is the
+    // parity this CTA waits for next; buffer 0 starts filled locally
+    uint32_t ph = 0;
+    bool skip_wait = true;
+    const uint32_t sbar_local = smem_addr(mbar + kRing);
+    auto wait_s = [&](int b) -> bool {
+        const bool ok = mbar_wait(sbar_local + 8u * b, (ph >> b) & 1u, kSpin);
+        ph ^= 1u << b;
+        return ok;
+    };
+    auto wait_copy = [&](uint32_t c) -> bool {
+        return mbar_wait(smem_addr(mbar + c % kRing), (c / kRing) & 1, kSpin);
+    };
+    auto issue = [&]() {  // thread 0: keep up to kRing milliseconds in flight
+        while (c_issue < c_cons + kRing && ms_next <= a.T) {
+            const uint32_t st = c_issue % kRing;
+            const uint32_t bar = smem_addr(mbar + st);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(10 * run_bytes)
+                         : "memory");
+            for (int sub = 0; sub < 10; sub++)
+                asm volatile(
+                    "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                        smem_addr(ring + ((size_t)st * 10 + sub) * R)),
+                    "l"(noise_bytes + (((size_t)ms_next * 10 + sub) * N + r0) * sizeof(float2)), "r"(run_bytes),
+                    "r"(bar)
+                    : "memory");
+            c_issue++;
+            ms_next++;
+        }
+    };
+    auto broadcast_flag = [&](int slot, int v) {  // flags[slot] of every CTA <- v
+        if (t < (int)csize) st_cluster_s32(map_rank(flags_local + 4u * slot, t), v);
+    };
+
+    while (ts <= a.T) {
+        if (t == 0) issue();
+        bool late = __syncthreads_or(!wait_copy(c_cons));
+        const int lslot = (int)(c_cons & 1) * 8;
+        const float2* nz = ring + (size_t)(c_cons % kRing) * 10 * R + (act ? t : 0);
+
+#pragma unroll 1
+        for (int sub = 0; sub < 10; sub++) {
+            if (!skip_wait && !late) late = !wait_s(cur);
+            skip_wait = false;
+            // all threads are past this phase (arm the buffer's next one), and
+            // the partial table of the previous substep has been read
+            __syncthreads();
+            if (t == 0 && !late)
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar_local + 8u * cur),
+                             "r"(4 * N)
+                             : "memory");
+            const float2* Sp = reinterpret_cast<const float2*>(S_buf + cur * NC + 2 * K2 * w);
+            float2 acc[RPL];
+#pragma unroll
+            for (int i = 0; i < RPL; i++) acc[i] = make_float2(0.f, 0.f);
+#pragma unroll
+            for (int j = 0; j < K2; j++) {
+                const float2 s2 = Sp[j];  // same address in every lane: broadcast
+#pragma unroll
+                for (int i = 0; i < RPL; i++) {
+                    const float2 m = (j < KRP) ? scr[i][j < KRP ? j : 0]
+                                               : SCs[((size_t)(w * RPL + i) * KS + (j - KRP)) * 32 + lane];
+                    acc[i] = __ffma2_rn(m, s2, acc[i]);
+                }
+            }
+#pragma unroll
+            for (int i = 0; i < RPL; i++) red[w * RP + lane + 32 * i] = acc[i].x + acc[i].y;
+            __syncthreads();
+            if (w < upd_warps) {
+                float coupling = 0.f;
+                for (int w2 = 0; w2 < W; w2++) coupling += red[w2 * RP + t];
+                const float2 n = act ? nz[(size_t)sub * R] : make_float2(0.f, 0.f);
+                IE = fmaf(GJ, coupling, fmaf(wEE, S_E, C::w_E__I_0)) - wIE * S_I;
+                II = fmaf(wEI, S_E, C::w_I__I_0) - S_I;
+                rE = rate(fmaf(C::a_E, IE, -C::b_E), C::d_E, 1.0f / C::d_E, -C::d_E * LOG2E);
+                rI = rate(fmaf(C::a_I, II, -C::b_I), C::d_I, 1.0f / C::d_I, -C::d_I * LOG2E);
+                const float aE = fmaf(-kDtGammaE, S_E, kDtGammaE);
+                const float dSE = fmaf(aE, rE, fmaf(-kDtInvTauE, S_E, SQ * n.x));
+                const float dSI = fmaf(kDtGammaI, rI, fmaf(-kDtInvTauI, S_I, SQ * n.y));
+                S_E = __saturatef(S_E + dSE);
+                S_I = __saturatef(S_I + dSI);
+                if (act) {  // to buffer cur^1 of every CTA; its mbarrier counts the bytes
+                    const uint32_t dst = s_local + (uint32_t)(((cur ^ 1) * NC + node) * sizeof(float));
+                    const uint32_t bar = sbar_local + 8u * (cur ^ 1);
+                    for (uint32_t r = 0; r < csize; r++) st_async_f32(map_rank(dst, r), S_E, map_rank(bar, r));
+                }
+            }
+            cur ^= 1;
+        }
+        // a late noise copy or S_E exchange anywhere stops the whole cluster
+        broadcast_flag(lslot + (int)crank, __syncthreads_or(late) ? 1 : 0);
+        cluster_sync();
+        bool any_late = false;
+        for (uint32_t r = 0; r < csize; r++) any_late |= flags[lslot + r] != 0;
+        if (any_late) {
+            timed_out = true;
+            break;
+        }
+        c_cons++;
+        bw.step(S_E);
+        if (--to_frame == 0) {  // ts % TR == 0
+            to_frame = a.TR;
+            if (act) {
+                a.bold[((size_t)sim * a.frames + frame) * N + node] = bw.bold();
+                if (frame >= a.n_vols_remove) {
+                    double* e = ext + t;
+                    e[0 * RP] += S_E;
+                    e[1 * RP] += IE;
+                    e[2 * RP] += rE;
+                    e[3 * RP] += S_I;
+                    e[4 * RP] += II;
+                    e[5 * RP] += rI;
+                }
+            }
+            frame++;
+        }
+        ts++;
+        if (adjusting) {
+            if (ts >= a.samp_start && ts <= a.samp_end) mean_IE += (double)IE;
+            if (ts == a.samp_end) {
+                bool needs = false;
+                if (act) {
+                    const double diff = mean_IE / duration - (double)C::b_a_ratio_E;
+                    if (fabs(diff + 0.026) > 0.005) {
+                        needs = true;
+                        if (trial < a.max_trials) {
+                            if (diff < -0.026) {
+                                wIE -= delta;
+                                delta = fmaxf(delta - 0.001f, 0.001f);
+                            } else {
+                                wIE += delta;
+                            }
+                        }
+                    }
+                }
+                broadcast_flag(16 + (int)crank, __syncthreads_or(needs) ? 1 : 0);
+                cluster_sync();
+                bool any = false;
+                for (uint32_t r = 0; r < csize; r++) any |= flags[16 + r] != 0;
+                if (any) {
+                    if (trial < a.max_trials) {
+                        S_E = S_I = 0.001f;
+                        bw = BW();
+                        mean_IE = 0.0;
+                        if (act)
+                            for (int e = 0; e < 6; e++) ext[e * RP + t] = 0.0;
+                        // the S_E the next substep would read is in flight: let it land,
+                        // then overwrite the buffer locally with the restart state
+                        bool lt = !wait_s(cur);
+                        skip_wait = true;
+                        __syncthreads();
+                        for (int k = t; k < N; k += blockDim.x) S_buf[cur * NC + k] = 0.001f;
+                        ts = 0;
+                        frame = 0;
+                        to_frame = 1;
+                        trial++;
+                        // copies in flight hold milliseconds after the restart point:
+                        // let them land, then refetch from millisecond 0 (thread 0
+                        // issues, so it publishes how far it got)
+                        if (t == 0) flags[24] = (int)c_issue;
+                        __syncthreads();
+                        const uint32_t in_flight_end = (uint32_t)flags[24];
+                        for (; c_cons < in_flight_end; c_cons++) lt |= !wait_copy(c_cons);
+                        ms_next = 0;
+                        if (lt && t == 0) atomicOr(a.status, kStatusTimeout);
+                    } else {
+                        failed = true;
+                        adjusting = false;
+                    }
+                } else {
+                    adjusting = false;
+                }
+                cluster_sync();  // fic flags may be rewritten only after every CTA read them
+            }
+        }
+    }
+    if (!timed_out && act) {
+        a.wIE_out[(size_t)sim * N + node] = (double)wIE;
+        const double kept = (double)(frame - a.n_vols_remove);
+        for (int e = 0; e < 6; e++) a.ext[((size_t)sim * 6 + e) * N + node] = ext[e * RP + t] / kept;
+    }
+    if (!timed_out && crank == 0 && t == 0) {
+        a.trials[sim] = trial;
+        a.failed[sim] = failed ? 1 : 0;
+    }
+    if (timed_out) {
+        if (t == 0) {
+            atomicOr(a.status, kStatusTimeout);
+            for (uint32_t c = c_cons; c < c_issue; c++) wait_copy(c);  // own copies land before exit
+        }
+        __syncthreads();
+    }
+    // the S_E sent at the last substep lands before anyone leaves: no CTA
+    // exits while another may still write its shared memory
+    if (!skip_wait) wait_s(cur);
+    cluster_sync();
+}
+
+// ---------------------------------------------------------------- launch
+
+struct Variant {
+    int rpl, k2, krp;
+    const void* fn;
+    size_t (*bytes)(int W, int R);
+};
+
+template <int RPL, int K2, int KRP>
+Variant make_variant() {
+    return {RPL, K2, KRP, (const void*)&integrate_colsplit_kernel<RPL, K2, KRP>, &ColLayout<RPL, K2, KRP>::bytes};
+}
+
+// rows per lane 2 or 4; column pairs per warp 8, 10, 13, 16, 25; all pairs
+// in registers, or 8 in registers and the rest in shared memory
+#define BNM_V(K2)                                                                                        \
+    make_variant<2, K2, K2>(), make_variant<4, K2, K2>(), make_variant<2, K2, (K2 < 8 ? K2 : 8)>(), \
+        make_variant<4, K2, (K2 < 8 ? K2 : 8)>()
+const std::vector<Variant>& variants() {
+    static const std::vector<Variant> v = {BNM_V(8), BNM_V(10), BNM_V(13), BNM_V(16), BNM_V(25)};
+    return v;
+}
+#undef BNM_V
+
+const Variant* find(int rpl, int k2, int krp) {
+    for (const Variant& v : variants())
+        if (v.rpl == rpl && v.k2 == k2 && v.krp == krp) return &v;
+    return nullptr;
+}
+
+}  // namespace
+}  // namespace bnm
+
+using namespace bnm;
+
+// Checks one column-split configuration for node count N: rows per CTA R
+// (even, at most 32 RPL, with a node in every rank), warps W = N / (2 K2)
+// rounded up (at least R threads), the kernel's own block-size limit and
+// shared memory.  Returns 1 and the launch shape when it can run.
+extern "C" int bnm_colsplit_shape(int N, int csize, int rpl, int k2, int krp, int* threads, int* rows, size_t* smem) {
+    if (N <= 0 || N > 512 || (N & 1) || csize < 1 || csize > 8) return 0;
+    const Variant* v = find(rpl, k2, krp);
+    if (!v) return 0;
+    int R = (N + csize - 1) / csize;
+    R += R & 1;  // bulk copies of the own nodes' noise need even node runs
+    if (R > 32 * rpl || (csize - 1) * R >= N) return 0;
+    const int W = (N + 2 * k2 - 1) / (2 * k2);
+    if (W * 32 < R || W * 32 > 1024) return 0;
+    cudaFuncAttributes fa;
+    if (cudaFuncGetAttributes(&fa, v->fn) != cudaSuccess) return 0;
+    if (W * 32 > fa.maxThreadsPerBlock) return 0;
+    const size_t sm = v->bytes(W, R);
+    if (sm > 227 * 1024) return 0;
+    *threads = W * 32;
+    *rows = R;
+    *smem = sm;
+    return 1;
+}
+
+// The (rows per lane, column pairs per warp, pairs in registers) variants built.
+extern "C" int bnm_colsplit_variants(int* out3, int max) {
+    int n = 0;
+    for (const Variant& v : variants()) {
+        if (n < max) {
+            out3[3 * n] = v.rpl;
+            out3[3 * n + 1] = v.k2;
+            out3[3 * n + 2] = v.krp;
+        }
+        n++;
+    }
+    return n;
+}
+
+cudaError_t bnm_launch_integrate_colsplit(const SimArgs& a, int csize, int rpl, int k2, int krp, cudaStream_t st) {
+    int threads = 0, R = 0;
+    size_t smem = 0;
+    if (!bnm_colsplit_shape(a.N, csize, rpl, k2, krp, &threads, &R, &smem)) return cudaErrorInvalidValue;
+    if (a.sc_ld < a.N) return cudaErrorInvalidValue;
+    const Variant* v = find(rpl, k2, krp);
+    cudaError_t e = cudaFuncSetAttribute(v->fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof cfg);
+    cfg.gridDim = dim3((unsigned)(a.n_sims * csize));
+    cfg.blockDim = dim3((unsigned)threads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = (unsigned)csize;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    int clusters = 0;
+    e = cudaOccupancyMaxActiveClusters(&clusters, v->fn, &cfg);
+    if (e != cudaSuccess) return e;
+    if (clusters < 1) return cudaErrorInvalidConfiguration;
+    void* args[] = {(void*)&a, (void*)&R};
+    return cudaLaunchKernelExC(&cfg, v->fn, args);
+}

@@ -402,6 +402,7 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
         }
     }
     if (sh.kind == 1) return bnm_launch_integrate_cluster(a, sh.csize, sh.rpw, sh.kr, st);
+    if (sh.kind == 3) return bnm_launch_integrate_colsplit(a, sh.csize, sh.rpw, sh.slots, sh.kr, st);
     if (sh.kind != 2) return cudaErrorInvalidValue;
     const int threads = ((a.N + 31) / 32) * 32;
     if (threads > 1024) return cudaErrorInvalidValue;
@@ -439,6 +440,18 @@ int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max) {
             size_t smem;
             if (bnm_cluster_shape(N, cs, shapes[v][0], shapes[v][1], &threads, &rows, &smem))
                 add({1, 0, cs, shapes[v][0], shapes[v][1]});
+        }
+    int vs[3 * 64];
+    const int nv = bnm_colsplit_variants(vs, 64);
+    for (int cs : {1, 2, 4, 8})
+        for (int v = 0; v < nv && v < 64; v++) {
+            int threads, rows;
+            size_t smem;
+            const int rpl = vs[3 * v], k2 = vs[3 * v + 1], krp = vs[3 * v + 2];
+            bool dup = false;  // the variant table repeats (rpl, k2, k2) when k2 <= 8
+            for (int u = 0; u < v; u++)
+                dup |= vs[3 * u] == rpl && vs[3 * u + 1] == k2 && vs[3 * u + 2] == krp;
+            if (!dup && bnm_colsplit_shape(N, cs, rpl, k2, krp, &threads, &rows, &smem)) add({3, k2, cs, rpl, krp});
         }
     add({2, 0, 0, 0, 0});
     return n < max ? n : max;

@@ -146,9 +146,12 @@ struct FicArgs {
 
 namespace bnm {
 // One FP32 integrator configuration.  kind 0: register-SC kernel (N <= 128)
-// with `slots` particles per CTA; kind 1: cluster kernel (N <= 512, even) with
-// `csize` CTAs per particle, `rpw` nodes per warp and `kr` SC column chunks in
-// registers; kind 2: the reference-order kernel in FP32 (any N).
+// with `slots` particles per CTA; kind 1: row-split cluster kernel (N <= 512,
+// even) with `csize` CTAs per particle, `rpw` nodes per warp and `kr` SC
+// column chunks in registers; kind 2: the reference-order kernel in FP32 (any
+// N); kind 3: column-split cluster kernel (N <= 512, even) with `csize` CTAs
+// per particle, `slots` column pairs per warp, `rpw` rows per lane and `kr`
+// column pairs in registers.
 struct IntegratorShape {
     int kind, slots, csize, rpw, kr;
 };
@@ -159,6 +162,9 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
 // Candidate shapes for N nodes (those that compile to a launchable kernel); returns the count.
 int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max);
 cudaError_t bnm_launch_integrate_cluster(const bnm::SimArgs& a, int csize, int rpw, int kr, cudaStream_t st);
+cudaError_t bnm_launch_integrate_colsplit(const bnm::SimArgs& a, int csize, int rpl, int k2, int krp, cudaStream_t st);
+extern "C" int bnm_colsplit_shape(int N, int csize, int rpl, int k2, int krp, int* threads, int* rows, size_t* smem);
+extern "C" int bnm_colsplit_variants(int* out3, int max);
 extern "C" int bnm_cluster_shape(int N, int csize, int rpw, int kr, int* threads, int* rows, size_t* smem);
 cudaError_t bnm_launch_integrate_exact(const bnm::SimArgs& a, int fp64, int num_sms, cudaStream_t st);
 cudaError_t bnm_launch_fc_window(const bnm::FcArgs& a, cudaStream_t st);

@@ -2,9 +2,11 @@
 oracle port, through the C ABI, in oracle-noise mode (the reference's
 mt19937 stream, bnm.cpp:38-43, fed to both).
 
-Every cluster shape the autotuner can pick is forced once (BNM_B200_SHAPE):
-1, 2, 4 and 8 CTAs per particle, 8 or 16 nodes per warp, and SC column chunks
-in registers only or split between registers and shared memory.  Bar, as for
+Every kind of cluster shape the autotuner can pick is forced once
+(BNM_B200_SHAPE): row-split (1, 2, 4 and 8 CTAs per particle, 8 or 16 nodes
+per warp) and column-split (2 or 4 rows per lane, 8 to 25 column pairs per
+warp), with SC in registers only or split between registers and shared
+memory.  Bar, as for
 the register kernel (N <= 128): on particles whose numerical FIC took the same
 decisions, BOLD within 1e-3 of its range, FC / FCD within 1e-3, cost within
 1e-2; wIE equal to the oracle's up to FP32 rounding.
@@ -24,10 +26,14 @@ SETUPS = {
     "n160": (160, 15000, 500, 2, 10, 2, 10, 3),
     "n400": (400, 11000, 500, 2, 6, 2, 2, 2),
 }
+# kind,slots,csize,rpw,kr: kind 1 row-split (rpw nodes per warp, kr chunks in registers); kind 3
+# column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers)
 SHAPES = {
-    "n160": ["1,0,1,8,4", "1,0,2,8,5", "1,0,4,16,4", "1,0,8,8,4"],
-    "n400": ["1,0,4,8,4", "1,0,8,8,8", "1,0,8,16,4"],
+    "n160": ["1,0,1,8,4", "1,0,2,8,5", "1,0,4,16,4", "1,0,8,8,4",
+             "3,10,2,4,10", "3,8,4,2,8", "3,13,2,4,8"],
+    "n400": ["1,0,4,8,4", "1,0,8,8,8", "1,0,8,16,4", "3,25,4,4,8", "3,13,8,2,13", "3,25,8,2,25"],
 }
+KINDS = {1: "cluster", 3: "colsplit"}
 
 
 @pytest.fixture(scope="module")
@@ -68,7 +74,9 @@ def test_cluster_shape_matches_fp64_oracle(name, shape, cases, monkeypatch):
     with B.Plan(c["cfg"], c["sc"], c["emp_fc"], c["emp_fcd"], host_noise=c["noise"]) as p:
         r = p.run(c["G"], c["wEE"], c["wEI"], c["wie0"] if not c["cfg"].do_fic else None)
         info = p.integrator()
-    assert info["kind"] == "cluster" and f'1,0,{info["csize"]},{info["rpw"]},{info["kr"]}' == shape
+    k = [int(v) for v in shape.split(",")]
+    assert info["kind"] == KINDS[k[0]], info
+    assert (info["slots"], info["csize"], info["rpw"], info["kr"]) == tuple(k[1:]), info
     same = (r["fic_ntrials"] == c["trials"]) & (np.abs(r["w_ie"] - c["wIE"]).max(1) < 1e-4)
     assert same.sum() >= 1, (r["fic_ntrials"], c["trials"])
     span = np.ptp(c["bold"], axis=1, keepdims=True) + 1e-12
@@ -86,5 +94,5 @@ def test_autotuner_picks_a_timed_cluster_shape(cases):
         info = p.integrator()
         r2 = p.run(c["G"], c["wEE"], c["wEI"])  # tuned once per batch size
         assert p.integrator() == info
-    assert info["kind"] == "cluster" and info["tried"] >= 4, info
+    assert info["kind"] in ("cluster", "colsplit") and info["tried"] >= 4, info
     np.testing.assert_array_equal(r1["cost"], r2["cost"])
