@@ -456,17 +456,3 @@ int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max) {
     add({2, 0, 0, 0, 0});
     return n < max ? n : max;
 }
-
-// FP32 launch without tuning: the register kernel (one slot, or BNM_B200_SLOTS)
-// when N <= 128, else the first cluster shape that fits, else the
-// reference-order kernel in float.
-cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStream_t st) {
-    using namespace bnm;
-    IntegratorShape c[16];
-    const int n = bnm_integrator_candidates(a.N, c, 16);
-    IntegratorShape s = c[0];
-    if (s.kind == 0)
-        if (const char* e = std::getenv("BNM_B200_SLOTS")) s.slots = std::atoi(e) == 2 ? 2 : 1;
-    (void)n;
-    return bnm_launch_integrate_shape(a, s, num_sms, st);
-}

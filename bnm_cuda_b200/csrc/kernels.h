@@ -156,7 +156,6 @@ struct IntegratorShape {
     int kind, slots, csize, rpw, kr;
 };
 }  // namespace bnm
-cudaError_t bnm_launch_integrate_f32(const bnm::SimArgs& a, int num_sms, cudaStream_t st);
 cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::IntegratorShape& s, int num_sms,
                                        cudaStream_t st);
 // Candidate shapes for N nodes (those that compile to a launchable kernel); returns the count.
