@@ -18,7 +18,11 @@
 //     32/RPW lanes);
 //   * two CTA barriers per substep: one after the S_E wait (all threads are
 //     past it before the buffer's next phase is armed, and the partial table
-//     of the previous substep has been read), one between partials and sums.
+//     of the previous substep has been read), one between partials and sums;
+//   * a cluster of one CTA (N up to 32 RPL, all of SC in registers) skips the
+//     asynchronous exchange: owners store S_E straight into the other buffer
+//     and the first barrier of the next substep orders it (the buffer being
+//     written was last read before that barrier of the previous substep).
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -55,7 +59,7 @@ struct ColLayout {
 
 template <int RPL, int K2, int KRP>
 __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
-    static_assert(RPL >= 1 && RPL <= 4, "RPL");
+    static_assert(RPL >= 1 && RPL <= 8, "RPL");
     static_assert(KRP >= 0 && KRP <= K2, "KRP");
     constexpr int KS = K2 - KRP;  // column pairs in shared memory
     constexpr int RP = 32 * RPL;
@@ -82,6 +86,7 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
 
     const int node = r0 + t;
     const bool act = t < r_own;  // thread t owns node r0 + t
+    const bool solo = csize == 1;  // S_E exchange through local shared memory
     const long long kSpin = 1ll << 26;
 
     cluster_sync();  // every CTA of the cluster runs before any distributed shared memory access
@@ -89,9 +94,10 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
         for (int b = 0; b < kRing + 2; b++)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(mbar + b)) : "memory");
         // buffer 1 receives S_E after the first substep: N values of 4 bytes
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar + kRing + 1)),
-                     "r"(4 * N)
-                     : "memory");
+        if (!solo)
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(mbar + kRing + 1)),
+                         "r"(4 * N)
+                         : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int k = t; k < 2 * NC; k += blockDim.x) S_buf[k] = (k % NC) < N ? 0.001f : 0.f;
@@ -185,12 +191,12 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
 
 #pragma unroll 1
         for (int sub = 0; sub < 10; sub++) {
-            if (!skip_wait && !late) late = !wait_s(cur);
+            if (!solo && !skip_wait && !late) late = !wait_s(cur);
             skip_wait = false;
             // all threads are past this phase (arm the buffer's next one), and
             // the partial table of the previous substep has been read
             __syncthreads();
-            if (t == 0 && !late)
+            if (!solo && t == 0 && !late)
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar_local + 8u * cur),
                              "r"(4 * N)
                              : "memory");
@@ -224,7 +230,9 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
                 const float dSI = fmaf(kDtGammaI, rI, fmaf(-kDtInvTauI, S_I, SQ * n.y));
                 S_E = __saturatef(S_E + dSE);
                 S_I = __saturatef(S_I + dSI);
-                if (act) {  // to buffer cur^1 of every CTA; its mbarrier counts the bytes
+                if (act && solo) {
+                    S_buf[(cur ^ 1) * NC + node] = S_E;
+                } else if (act) {  // to buffer cur^1 of every CTA; its mbarrier counts the bytes
                     const uint32_t dst = s_local + (uint32_t)(((cur ^ 1) * NC + node) * sizeof(float));
                     const uint32_t bar = sbar_local + 8u * (cur ^ 1);
                     for (uint32_t r = 0; r < csize; r++) st_async_f32(map_rank(dst, r), S_E, map_rank(bar, r));
@@ -291,8 +299,11 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
                             for (int e = 0; e < 6; e++) ext[e * RP + t] = 0.0;
                         // the S_E the next substep would read is in flight: let it land,
                         // then overwrite the buffer locally with the restart state
-                        bool lt = !wait_s(cur);
-                        skip_wait = true;
+                        bool lt = false;
+                        if (!solo) {
+                            lt = !wait_s(cur);
+                            skip_wait = true;
+                        }
                         __syncthreads();
                         for (int k = t; k < N; k += blockDim.x) S_buf[cur * NC + k] = 0.001f;
                         ts = 0;
@@ -337,7 +348,7 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
     }
     // the S_E sent at the last substep lands before anyone leaves: no CTA
     // exits while another may still write its shared memory
-    if (!skip_wait) wait_s(cur);
+    if (!solo && !skip_wait) wait_s(cur);
     cluster_sync();
 }
 
@@ -355,12 +366,16 @@ Variant make_variant() {
 }
 
 // rows per lane 2 or 4; column pairs per warp 8, 10, 13, 16, 25; all pairs
-// in registers, or 8 in registers and the rest in shared memory
+// in registers, or 8 in registers and the rest in shared memory.  Plus
+// row-heavy shapes with all of SC in registers for one-CTA clusters up to
+// N = 160 / 192 / 208 (5, 6, 7 rows per lane).
 #define BNM_V(K2)                                                                                        \
     make_variant<2, K2, K2>(), make_variant<4, K2, K2>(), make_variant<2, K2, (K2 < 8 ? K2 : 8)>(), \
         make_variant<4, K2, (K2 < 8 ? K2 : 8)>()
 const std::vector<Variant>& variants() {
-    static const std::vector<Variant> v = {BNM_V(8), BNM_V(10), BNM_V(13), BNM_V(16), BNM_V(25)};
+    static const std::vector<Variant> v = {BNM_V(8),  BNM_V(10), BNM_V(13), BNM_V(16), BNM_V(25),
+                                           make_variant<5, 10, 10>(), make_variant<6, 12, 12>(),
+                                           make_variant<7, 13, 13>()};
     return v;
 }
 #undef BNM_V

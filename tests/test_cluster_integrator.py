@@ -4,9 +4,9 @@ mt19937 stream, bnm.cpp:38-43, fed to both).
 
 Every kind of cluster shape the autotuner can pick is forced once
 (BNM_B200_SHAPE): row-split (1, 2, 4 and 8 CTAs per particle, 8 or 16 nodes
-per warp) and column-split (2 or 4 rows per lane, 8 to 25 column pairs per
-warp), with SC in registers only or split between registers and shared
-memory.  Bar, as for
+per warp) and column-split (2 to 7 rows per lane, 8 to 25 column pairs per
+warp, one-CTA clusters with a local S_E exchange included), with SC in
+registers only or split between registers and shared memory.  Bar, as for
 the register kernel (N <= 128): on particles whose numerical FIC took the same
 decisions, BOLD within 1e-3 of its range, FC / FCD within 1e-3, cost within
 1e-2; wIE equal to the oracle's up to FP32 rounding.
@@ -30,7 +30,9 @@ SETUPS = {
 # column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers)
 SHAPES = {
     "n160": ["1,0,1,8,4", "1,0,2,8,5", "1,0,4,16,4", "1,0,8,8,4",
-             "3,10,2,4,10", "3,8,4,2,8", "3,13,2,4,8"],
+             "3,10,2,4,10", "3,8,4,2,8", "3,13,2,4,8",
+             # one-CTA clusters: S_E exchanged through local shared memory
+             "3,10,1,5,10", "3,12,1,6,12", "3,13,1,7,13"],
     "n400": ["1,0,4,8,4", "1,0,8,8,8", "1,0,8,16,4", "3,25,4,4,8", "3,13,8,2,13", "3,25,8,2,25"],
 }
 KINDS = {1: "cluster", 3: "colsplit"}
