@@ -57,7 +57,8 @@ class _Sizes(C.Structure):
 
 class _BatchOut(C.Structure):
     _fields_ = [(k, C.c_void_p) for k in ("cost", "fic_penalty", "fc_corr", "fc_diff", "fcd_ks", "w_ie", "fic_failed",
-                                          "fic_ntrials", "fic_unstable", "ext_means", "bold", "fc", "fcd")]
+                                          "fic_ntrials", "fic_unstable", "ext_means", "bold", "fc", "fcd",
+                                          "fcd_left", "fcd_right")]
 
 
 class _CmaesParams(C.Structure):
@@ -221,7 +222,7 @@ class Plan:
         for k in ("fic_failed", "fic_ntrials", "fic_unstable"):
             res[k] = np.zeros(n, np.int32)
         shapes = {"w_ie": (n, N), "ext_means": (n, 6, N), "bold": (n, s["frames"], N), "fc": (n, s["n_pairs"]),
-                  "fcd": (n, s["n_fcd"])}
+                  "fcd": (n, s["n_fcd"]), "fcd_left": (n, s["n_fcd"]), "fcd_right": (n, s["n_fcd"])}
         for k in outputs:
             res[k] = np.zeros(shapes[k])
         o = _BatchOut()
@@ -240,7 +241,8 @@ class Plan:
             raise ValueError(f"bold must be [n, {s['corr_len']}, {self.cfg.nodes}]")
         n = bold.shape[0]
         res = {k: np.zeros(n) for k in ("cost", "fic_penalty", "fc_corr", "fc_diff", "fcd_ks")}
-        shapes = {"fc": (n, s["n_pairs"]), "fcd": (n, s["n_fcd"])}
+        shapes = {"fc": (n, s["n_pairs"]), "fcd": (n, s["n_fcd"]), "fcd_left": (n, s["n_fcd"]),
+                  "fcd_right": (n, s["n_fcd"])}
         for k in outputs:
             res[k] = np.zeros(shapes[k])
         o = _BatchOut()

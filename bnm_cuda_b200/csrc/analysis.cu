@@ -186,13 +186,13 @@ __global__ void __launch_bounds__(256) fcd_gram_kernel(FcdArgs a) {
     if (threadIdx.x < kTile) {
         const int r = a0 + threadIdx.x;
         double m = 0, s = 0;
-        if (r < a.W) window_norm(ws + 2 * r, a.P, m, s);
+        if (r < a.W) window_norm(ws + 2 * r, a.p1 - a.p0, m, s);
         mA[threadIdx.x] = m;
         sA[threadIdx.x] = s;
     } else if (threadIdx.x < 2 * kTile) {
         const int r = b0 + threadIdx.x - kTile;
         double m = 0, s = 0;
-        if (r < a.W) window_norm(ws + 2 * r, a.P, m, s);
+        if (r < a.W) window_norm(ws + 2 * r, a.p1 - a.p0, m, s);
         mB[threadIdx.x - kTile] = m;
         sB[threadIdx.x - kTile] = s;
     }
@@ -203,14 +203,14 @@ __global__ void __launch_bounds__(256) fcd_gram_kernel(FcdArgs a) {
     for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < 4; j++) acc[i][j] = 0.f;
-    for (int k0 = 0; k0 < a.P; k0 += kTk) {
+    for (int k0 = a.p0; k0 < a.p1; k0 += kTk) {
         // load 64 rows x 16 columns of A and B, normalised on the fly
         for (int e = threadIdx.x; e < kTile * kTk; e += blockDim.x) {
             const int r = e / kTk, c = e % kTk;
             const int ra = a0 + r, rb = b0 + r, col = k0 + c;
             float va = 0.f, vb = 0.f;
-            if (ra < a.W && col < a.P) va = (float)(((double)V[(size_t)ra * a.P + col] - mA[r]) * sA[r]);
-            if (rb < a.W && col < a.P) vb = (float)(((double)V[(size_t)rb * a.P + col] - mB[r]) * sB[r]);
+            if (ra < a.W && col < a.p1) va = (float)(((double)V[(size_t)ra * a.P + col] - mA[r]) * sA[r]);
+            if (rb < a.W && col < a.p1) vb = (float)(((double)V[(size_t)rb * a.P + col] - mB[r]) * sB[r]);
             As[c][r] = va;
             Bs[c][r] = vb;
         }
@@ -230,8 +230,8 @@ __global__ void __launch_bounds__(256) fcd_gram_kernel(FcdArgs a) {
         __syncthreads();
     }
     bool any_nan = false;
-    unsigned int* hist = a.hist + (size_t)sim * (a.m + 1);
-    unsigned int* eq = a.eq + (size_t)sim * (a.m + 1);
+    unsigned int* hist = a.hist ? a.hist + (size_t)sim * (a.m + 1) : nullptr;
+    unsigned int* eq = a.hist ? a.eq + (size_t)sim * (a.m + 1) : nullptr;
 #pragma unroll
     for (int i = 0; i < 4; i++)
 #pragma unroll
@@ -242,17 +242,19 @@ __global__ void __launch_bounds__(256) fcd_gram_kernel(FcdArgs a) {
                 if (!(v == v) || isinf(v)) { any_nan = true; continue; }
                 const size_t idx = (size_t)wa * (wa - 1) / 2 + wb;
                 if (a.fcd) a.fcd[(size_t)sim * a.n_fcd + idx] = v;
-                int c;
-                bool equal;
-                if (a.ks_lut)
-                    ks_bucket_lut(a.emp_sorted, a.ks_lut, a.m, (double)v, c, equal);
-                else
-                    ks_bucket(a.emp_sorted, a.m, (double)v, c, equal);
-                atomicAdd(&hist[c], 1u);
-                if (equal) atomicAdd(&eq[c], 1u);
+                if (hist) {
+                    int c;
+                    bool equal;
+                    if (a.ks_lut)
+                        ks_bucket_lut(a.emp_sorted, a.ks_lut, a.m, (double)v, c, equal);
+                    else
+                        ks_bucket(a.emp_sorted, a.m, (double)v, c, equal);
+                    atomicAdd(&hist[c], 1u);
+                    if (equal) atomicAdd(&eq[c], 1u);
+                }
             }
         }
-    if (any_nan) atomicOr(&a.nan_flag[sim], 1);
+    if (any_nan && a.nan_flag) atomicOr(&a.nan_flag[sim], 1);
 }
 
 // ------------------------------------------------------------ KS + GOF
@@ -374,6 +376,45 @@ static cudaError_t launch_fc_window(const FcArgs& a, const TB* bold, cudaStream_
 
 cudaError_t bnm_launch_fc_window(const FcArgs& a, cudaStream_t st) {
     return a.bold_f64 ? launch_fc_window<double>(a, a.bold_f64, st) : launch_fc_window<float>(a, a.bold, st);
+}
+
+// Window-FC sums over a pair range, one CTA per (window, simulation): the
+// centring of the hemisphere FCDs (window_fc_stats with save_hemis,
+// bnm.cu:436-496).
+__global__ void __launch_bounds__(256) window_sums_kernel(const float* wfc, int W, int P, int p0, int p1,
+                                                          double* out) {
+    __shared__ double sh[16];
+    const int w = blockIdx.x, sim = blockIdx.y;
+    const float* v = wfc + ((size_t)sim * W + w) * P;
+    double s = 0.0, ss = 0.0;
+    for (int p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+        const double x = v[p];
+        s += x;
+        ss += x * x;
+    }
+    s = warp_sum(s);
+    ss = warp_sum(ss);
+    if ((threadIdx.x & 31) == 0) {
+        sh[threadIdx.x >> 5] = s;
+        sh[8 + (threadIdx.x >> 5)] = ss;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+            a += sh[k];
+            b += sh[8 + k];
+        }
+        out[((size_t)sim * W + w) * 2] = a;
+        out[((size_t)sim * W + w) * 2 + 1] = b;
+    }
+}
+
+cudaError_t bnm_launch_window_sums(const float* wfc, int n_sims, int W, int P, int p0, int p1, double* wsum_out,
+                                   cudaStream_t st) {
+    if (p0 < 0 || p1 > P || p1 - p0 < 2) return cudaErrorInvalidValue;
+    window_sums_kernel<<<dim3(W, n_sims), 256, 0, st>>>(wfc, W, P, p0, p1, wsum_out);
+    return cudaGetLastError();
 }
 
 cudaError_t bnm_launch_fcd(FcdArgs a, cudaStream_t st) {

@@ -158,6 +158,9 @@ struct bnm_plan {
     unsigned char *d_fcd_hi = nullptr, *d_fcd_lo = nullptr, *d_fc_hi = nullptr, *d_fc_lo = nullptr;
     int* d_tril_map = nullptr;
     int fcd_rb = 0, fcd_kb = 0, fc_rb = 0, fc_kb = 0, gram_chunk = 0;
+    // hemisphere FCDs (optional outputs; allocated on first request)
+    float* d_fcd_hemi = nullptr;
+    double* d_wsum_hemi = nullptr;
     // FP32 integrator picked by the autotuner for batches of tuned_n particles
     IntegratorShape shape{};
     int tuned_n = 0, n_tried = 0;
@@ -524,7 +527,19 @@ static cudaError_t rec(bnm_plan* p, cudaEvent_t e) {
 
 // FC + window FC (+ tensor-core FC Gram), FCD + KS histogram, goodness of
 // fit, on the plan's BOLD buffer; events 3, 4, 5 close the stages.
-static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
+// Hemisphere FCD buffers, allocated the first time a caller asks for them.
+static int ensure_hemi(bnm_plan* p) {
+    if (p->d_fcd_hemi) return BNM_OK;
+    const int N = p->cfg.nodes, h = N / 2;
+    if (p->cfg.no_fcd || h * (h - 1) / 2 < 2)
+        return fail(BNM_EINVAL, "hemisphere FCDs need FCD and at least 3 nodes per hemisphere");
+    const size_t n = p->cfg.max_sims, W = std::max(p->sz.n_windows, 1);
+    BNM_CUDA_TRY(dalloc(p, &p->d_fcd_hemi, 2 * n * std::max(p->sz.n_fcd, 1)));
+    BNM_CUDA_TRY(dalloc(p, &p->d_wsum_hemi, 2 * n * W * 2));
+    return BNM_OK;
+}
+
+static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty, bool hemis = false) {
     const bnm_config& c = p->cfg;
     const bnm_sizes& s = p->sz;
     const int N = c.nodes;
@@ -638,12 +653,39 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty) {
         da.n_fcd = s.n_fcd;
         da.emp_sorted = p->d_emp_sorted;
         da.ks_lut = p->d_ks_lut;
+        da.p0 = 0;
+        da.p1 = s.n_pairs;
         da.m = p->m;
         da.hist = p->d_hist;
         da.eq = p->d_eq;
         da.nan_flag = p->d_nan;
         BNM_CUDA_TRY(bnm_launch_fcd(da, st));
         p->launches++;
+    }
+    if (hemis) {
+        // left / right hemisphere FCD over the first / last (N/2)(N/2-1)/2 pairs,
+        // each centred over its own pairs (window_fc_stats + fcd with save_hemis,
+        // bnm.cu:436-551); not part of the cost
+        const int h = N / 2, nh = h * (h - 1) / 2;
+        const size_t W = std::max(s.n_windows, 1), nmax = c.max_sims;
+        for (int side = 0; side < 2; side++) {
+            const int p0 = side == 0 ? 0 : s.n_pairs - nh, p1 = side == 0 ? nh : s.n_pairs;
+            double* ws = p->d_wsum_hemi + side * nmax * W * 2;
+            BNM_CUDA_TRY(bnm_launch_window_sums(p->d_wfc, n, s.n_windows, s.n_pairs, p0, p1, ws, st));
+            FcdArgs da;
+            std::memset(&da, 0, sizeof da);
+            da.n_sims = n;
+            da.W = s.n_windows;
+            da.P = s.n_pairs;
+            da.wfc = p->d_wfc;
+            da.wsum = ws;
+            da.fcd = p->d_fcd_hemi + side * nmax * s.n_fcd;
+            da.n_fcd = s.n_fcd;
+            da.p0 = p0;
+            da.p1 = p1;
+            BNM_CUDA_TRY(bnm_launch_fcd(da, st));
+            p->launches += 2;
+        }
     }
     BNM_CUDA_TRY(rec(p, p->ev[4]));
 
@@ -710,6 +752,11 @@ static int finish(bnm_plan* p, int n, bnm_batch_out* out, bool integrated) {
     }
     if ((rc = f2d(out->fc, p->d_fc, (size_t)n * s.n_pairs, st))) return rc;
     if (!c.no_fcd && (rc = f2d(out->fcd, p->d_fcd, (size_t)n * s.n_fcd, st))) return rc;
+    if (p->d_fcd_hemi) {
+        const size_t nmax = c.max_sims;
+        if ((rc = f2d(out->fcd_left, p->d_fcd_hemi, (size_t)n * s.n_fcd, st))) return rc;
+        if ((rc = f2d(out->fcd_right, p->d_fcd_hemi + nmax * s.n_fcd, (size_t)n * s.n_fcd, st))) return rc;
+    }
     BNM_CUDA_TRY(cudaStreamSynchronize(st));
     float ms;
     for (int i = 0; i < 5; i++) {
@@ -772,8 +819,10 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     const int N = c.nodes;
     if (!c.do_fic && !w_ie) return fail(BNM_EINVAL, "w_ie is required when do_fic == 0");
     BNM_CUDA_TRY(cudaSetDevice(c.device));
-    int rc = upload_params(p, n, G, w_ee, w_ei);
+    const bool hemis = out->fcd_left || out->fcd_right;
+    int rc = hemis ? ensure_hemi(p) : BNM_OK;
     if (rc) return rc;
+    if ((rc = upload_params(p, n, G, w_ee, w_ei))) return rc;
     cudaStream_t st = p->st;
     BNM_CUDA_TRY(cudaEventRecord(p->ev[0], st));
     const bool device_fic = c.do_fic && !w_ie;
@@ -806,7 +855,7 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     else
         BNM_CUDA_TRY(bnm_launch_integrate_exact(a, c.precision == BNM_PREC_F64, p->num_sms, st));
     BNM_CUDA_TRY(cudaEventRecord(p->ev[2], st));
-    if ((rc = launch_analysis(p, n, c.calculate_fic_penalty))) return rc;
+    if ((rc = launch_analysis(p, n, c.calculate_fic_penalty, hemis))) return rc;
     return finish(p, n, out, true);
 }
 
@@ -845,7 +894,10 @@ extern "C" int bnm_check_fit_bold(bnm_plan* p, int32_t n, const double* bold, bn
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_eq, 0, (size_t)n * (p->m + 1) * 4, st));
     for (int e = 0; e < 3; e++) BNM_CUDA_TRY(cudaEventRecord(p->ev[e], st));
     p->launches = 0;
-    int rc = launch_analysis(p, n, 0);
+    const bool hemis = out->fcd_left || out->fcd_right;
+    int rc = hemis ? ensure_hemi(p) : BNM_OK;
+    if (rc) return rc;
+    rc = launch_analysis(p, n, 0, hemis);
     if (rc) return rc;
     return finish(p, n, out, false);
 }

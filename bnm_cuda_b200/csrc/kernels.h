@@ -29,11 +29,12 @@ struct FcdArgs {
     int n_fcd;
     const double* emp_sorted;  // [m] ascending
     int m;
-    unsigned int* hist;     // [n][m+1] counts by upper_bound rank
+    unsigned int* hist;     // [n][m+1] counts by upper_bound rank, or null (no KS)
     unsigned int* eq;       // [n][m+1] sim values equal to emp_sorted[c-1]
     const int* ks_lut;      // bucket table of emp_sorted (kKsBuckets + 1), or null
     int* nan_flag;
     int tiles;              // tiles per side
+    int p0, p1;             // pair range [p0, p1) of the window-FC rows (wsum holds its sums)
 };
 
 struct GofArgs {
@@ -168,6 +169,10 @@ extern "C" int bnm_cluster_shape(int N, int csize, int rpw, int kr, int* threads
 cudaError_t bnm_launch_integrate_exact(const bnm::SimArgs& a, int fp64, int num_sms, cudaStream_t st);
 cudaError_t bnm_launch_fc_window(const bnm::FcArgs& a, cudaStream_t st);
 cudaError_t bnm_launch_fcd(bnm::FcdArgs a, cudaStream_t st);
+// Per-window sum and sum of squares of window FC over pairs [p0, p1) (FP64):
+// wsum_out [n][W][2].
+cudaError_t bnm_launch_window_sums(const float* wfc, int n_sims, int W, int P, int p0, int p1, double* wsum_out,
+                                   cudaStream_t st);
 cudaError_t bnm_launch_gof(const bnm::GofArgs& a, cudaStream_t st);
 cudaError_t bnm_launch_fcd_operand(const bnm::OperandArgs& a, cudaStream_t st);
 cudaError_t bnm_launch_fc_operand(const bnm::OperandArgs& a, cudaStream_t st);

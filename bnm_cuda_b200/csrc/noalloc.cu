@@ -200,6 +200,8 @@ extern "C" int bnm_gof_noalloc(const float* d_bold, int32_t n, int32_t frames, i
     da.hist = reinterpret_cast<unsigned int*>(s + o_hist);
     da.eq = reinterpret_cast<unsigned int*>(s + o_eq);
     da.nan_flag = fa.nan_flag;
+    da.p0 = 0;
+    da.p1 = P;
     BNM_CUDA_TRY(bnm_launch_fcd(da, st));
 
     GofArgs ga;

@@ -132,6 +132,9 @@ typedef struct bnm_batch_out {
     double *bold;        /* [n][frames][nodes] */
     double *fc;          /* [n][n_pairs] */
     double *fcd;         /* [n][n_fcd] */
+    double *fcd_left;    /* [n][n_fcd] FCD over the first (nodes/2)(nodes/2-1)/2 pairs (left hemisphere) and */
+    double *fcd_right;   /* [n][n_fcd] over the last as many (right): the reference's save_hemis outputs,
+                            bnm.cu:436-551; computed only when set, not part of the cost */
 } bnm_batch_out;
 
 /* One batch (a CMA-ES generation): integrate, BOLD, FC, window FC, FCD, KS,

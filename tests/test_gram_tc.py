@@ -127,3 +127,46 @@ def test_check_fit_bold_reproduces_the_batch_and_the_oracle(port):
         for i in range(n):
             ref = port.port_gof(r["bold"][i][nvr:], step, ws, emp_fc, emp_fcd, exc=exc)
             assert f["cost"][i] == pytest.approx(ref["cost"], abs=TOL[gram][2] + 1e-3)
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_hemisphere_fcd_against_fp64_oracle(case, port):
+    """fcd_left / fcd_right (the reference's save_hemis outputs, bnm.cu:436-551):
+    FCD over the first and the last (N/2)(N/2-1)/2 pairs of the window-FC
+    vectors, each centred over its own pairs, against FP64 from the oracle's
+    window FC (FP32 Gram: 1e-4).  Asking for them leaves the batch's FCD and
+    cost unchanged, and bnm_check_fit_bold returns the same values."""
+    N, T, TR, ws, step, remove, exc = CASES[case]
+    sc = synth.make_sc(N, 0.3, 5)
+    n = 2
+    G, wEE, wEI = synth.uniform_params(n, N, seed=14)
+    rng = np.random.default_rng(8)
+    emp_fc = rng.uniform(-0.2, 0.8, synth.n_pairs(N, exc))
+    emp_fcd = rng.uniform(-0.3, 1.0, 1000)
+    cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TR, window_size=ws, window_step=step,
+                   bold_remove_s=remove, exc_interhem=exc)
+    nvr = cfg.sizes()["n_vols_remove"]
+    with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+        plain = p.run(G, wEE, wEI, outputs=("fcd",))
+        r = p.run(G, wEE, wEI, outputs=("bold", "fcd", "fcd_left", "fcd_right"))
+        f = p.check_fit_bold(r["bold"][:, nvr:], outputs=("fcd_left", "fcd_right"))
+    np.testing.assert_array_equal(r["fcd"], plain["fcd"])
+    np.testing.assert_array_equal(r["cost"], plain["cost"])
+    np.testing.assert_array_equal(f["fcd_left"], r["fcd_left"])
+    np.testing.assert_array_equal(f["fcd_right"], r["fcd_right"])
+    h = N // 2
+    nh = h * (h - 1) // 2
+    for i in range(n):
+        kept = r["bold"][i][nvr:]
+        _, wfc = port.port_fcd_tril(kept, step, ws, exc=exc, window_fc=True)
+        P = wfc.shape[1]
+        for sub, got in ((wfc[:, :nh], r["fcd_left"][i]), (wfc[:, P - nh:], r["fcd_right"][i])):
+            z = sub - sub.mean(1, keepdims=True)
+            z /= np.sqrt((z * z).sum(1, keepdims=True))
+            a, b = np.tril_indices(len(z), -1)
+            assert np.abs(got - (z @ z.T)[a, b]).max() <= 1e-4
+        if exc:  # then the two ranges are exactly the within-hemisphere pairs
+            left = port.port_fcd_tril(kept[:, :h], step, ws, exc=False)
+            right = port.port_fcd_tril(kept[:, h:], step, ws, exc=False)
+            assert np.abs(r["fcd_left"][i] - left).max() <= 1e-4
+            assert np.abs(r["fcd_right"][i] - right).max() <= 1e-4
