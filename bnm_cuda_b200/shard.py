@@ -1,8 +1,8 @@
 """Particle sharding over ranks (one process per GPU).
 
 Particles of a generation are independent apart from the shared SC, noise
-table and targets (SURVEY of the reference: run_simulations treats each
-particle alone, bnm.cu:594-769), so a generation of ``n`` particles splits
+table and targets (the reference's run_simulations treats each particle
+alone, bnm.cu:594-769), so a generation of ``n`` particles splits
 into contiguous shards, one per rank, with no data-path collective.  The only
 exchange is the one a host CMA-ES needs after the generation: every rank's
 fit terms gathered, in particle order, on every rank.

@@ -1,7 +1,8 @@
 /*
  * TEST INFRASTRUCTURE ONLY (oracle).  This project's CPU restatement of the
  * reference's simulate-and-fit path, used by tests/, by smoke() and by the
- * CPU-baseline leg of bench.py as the checker.  The product never links it.
+ * CPU-baseline leg of bench.py to check the device results.  The product never
+ * links it.
  *
  * It follows the reference's CPU path (bnm.cpp, check_fit.cpp, fic.cpp):
  *   port_noise            run_CMAES.cpp:643-654 / bnm.cpp:38-43 noise stream

@@ -12,7 +12,7 @@ Tolerances:
     ulp); FIC trial counts and failure flags exact; FC to 1e-6 and FCD
     (window FC and the FCD Gram are FP32 on the device: 1e-4); cost to 1e-4.
   * FP32 product kernel vs the FP64 reference: BOLD to 1e-3 of its range,
-    FC / FCD within 1e-3 absolute, cost to 1e-2, on the
+    FC / FCD within 1e-3 absolute (the bar the FP32 product path is held to), cost to 1e-2, on the
     particles whose numerical FIC took the same decisions (see _same_fic_path).
 """
 import numpy as np
