@@ -180,7 +180,19 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
         }
     };
     auto broadcast_flag = [&](int slot, int v) {  // flags[slot] of every CTA <- v
-        if (t < (int)csize) st_cluster_s32(map_rank(flags_local + 4u * slot, t), v);
+        if (solo) {
+            if (t == 0) flags[slot] = v;
+        } else if (t < (int)csize) {
+            st_cluster_s32(map_rank(flags_local + 4u * slot, t), v);
+        }
+    };
+    // cluster-wide agreement point: a one-CTA cluster needs only a block
+    // barrier (no release fence at cluster scope)
+    auto agree = [&]() {
+        if (solo)
+            __syncthreads();
+        else
+            cluster_sync();
     };
 
     while (ts <= a.T) {
@@ -242,7 +254,7 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
         }
         // a late noise copy or S_E exchange anywhere stops the whole cluster
         broadcast_flag(lslot + (int)crank, __syncthreads_or(late) ? 1 : 0);
-        cluster_sync();
+        agree();
         bool any_late = false;
         for (uint32_t r = 0; r < csize; r++) any_late |= flags[lslot + r] != 0;
         if (any_late) {
@@ -287,7 +299,7 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
                     }
                 }
                 broadcast_flag(16 + (int)crank, __syncthreads_or(needs) ? 1 : 0);
-                cluster_sync();
+                agree();
                 bool any = false;
                 for (uint32_t r = 0; r < csize; r++) any |= flags[16 + r] != 0;
                 if (any) {
@@ -326,7 +338,7 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
                 } else {
                     adjusting = false;
                 }
-                cluster_sync();  // fic flags may be rewritten only after every CTA read them
+                agree();  // fic flags may be rewritten only after every CTA read them
             }
         }
     }
