@@ -41,6 +41,14 @@ namespace bnm {
 namespace {
 
 constexpr int kRing = 4;  // noise ring stages (milliseconds)
+// A late noise copy or S_E exchange is agreed on cluster-wide every kAgreeMs
+// milliseconds (and at the FIC decision and the last millisecond), not every
+// millisecond: a CTA that saw a wait run out stops issuing copies and waiting
+// but keeps computing and sending until the next agreement point, so every
+// CTA reaches the same points.  A CTA that stopped arming its S_E barriers
+// collects at most kAgreeMs * 5 * 4 N <= 163840 bytes of negative tx-count
+// per barrier (N <= 512), inside the mbarrier's 2^20 - 1 range.
+constexpr int kAgreeMs = 16;
 
 // Shared-memory layout (bytes), in this order:
 //   S      [2][32 KC] float          S_E of every node, double buffered
@@ -192,10 +200,11 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
         if (threadIdx.x < csize) st_cluster_s32(map_rank(flags_local + 4u * slot, threadIdx.x), v);
     };
 
+    bool late = false;  // sticky; block-uniform after each __syncthreads_or
+    int since_agree = 0, n_agree = 0;
     while (ts <= a.T) {
-        if (threadIdx.x == 0) issue();
-        bool late = __syncthreads_or(!wait_copy(c_cons));
-        const int lslot = (int)(c_cons & 1) * 8;
+        if (threadIdx.x == 0 && !late) issue();
+        late = __syncthreads_or(late || !wait_copy(c_cons));
         const float2* nz = ring + (size_t)(c_cons % kRing) * 10 * R + (act ? lr : 0);
 
 #pragma unroll 1
@@ -263,14 +272,20 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
             }
             cur ^= 1;
         }
-        // a late noise copy or S_E exchange anywhere stops the whole cluster
-        broadcast_flag(lslot + (int)crank, __syncthreads_or(late) ? 1 : 0);
-        cluster_sync();
-        bool any_late = false;
-        for (uint32_t t = 0; t < csize; t++) any_late |= flags[lslot + t] != 0;
-        if (any_late) {
-            timed_out = true;
-            break;
+        // a late noise copy or S_E exchange anywhere stops the whole cluster at
+        // the next agreement point (ts, adjusting and the counters are the
+        // same in every CTA, so all of them stop here together)
+        if (++since_agree == kAgreeMs || ts == a.T || (adjusting && ts + 1 == a.samp_end)) {
+            since_agree = 0;
+            const int lslot = (n_agree++ & 1) * 8;
+            broadcast_flag(lslot + (int)crank, __syncthreads_or(late) ? 1 : 0);
+            cluster_sync();
+            bool any_late = false;
+            for (uint32_t t = 0; t < csize; t++) any_late |= flags[lslot + t] != 0;
+            if (any_late) {
+                timed_out = true;
+                break;
+            }
         }
         c_cons++;
         bw.step(S_E);
@@ -363,7 +378,9 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
     if (timed_out) {
         if (threadIdx.x == 0) {
             atomicOr(a.status, kStatusTimeout);
-            for (uint32_t c = c_cons; c < c_issue; c++) wait_copy(c);  // own copies land before exit
+            // own copies land before exit: once a wait ran out no copy was
+            // issued, so only the last one of each ring stage can be in flight
+            for (uint32_t c = c_issue > (uint32_t)kRing ? c_issue - kRing : 0; c < c_issue; c++) wait_copy(c);
         }
         __syncthreads();
     }
