@@ -275,7 +275,7 @@ class Plan:
         """FP32 integrator shape the autotuner picked for the last batch size."""
         o, t = np.zeros(5, np.int32), C.c_int32()
         _check(lib().bnm_plan_integrator(self._h, _ptr(o), C.byref(t)))
-        kind = ["register", "cluster", "reference-order", "colsplit"][int(o[0])]
+        kind = ["register", "cluster", "reference-order", "colsplit", "colsplit2"][int(o[0])]
         return dict(kind=kind, slots=int(o[1]), csize=int(o[2]), rpw=int(o[3]), kr=int(o[4]), tried=t.value)
 
     def noise(self, offset: int, n: int) -> np.ndarray:

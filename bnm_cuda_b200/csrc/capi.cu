@@ -429,10 +429,15 @@ static int upload_params(bnm_plan* p, int n, const double* G, const double* w_ee
 // Autotuner of the FP32 integrator: times every candidate shape of
 // bnm_integrator_candidates on this batch size over 200 simulated
 // milliseconds without FIC (the per-millisecond cost does not depend on the
-// model time) and keeps the fastest.  BNM_B200_SHAPE="kind,slots,csize,rpw,kr"
+// model time) and keeps the fastest.  With `share` (plans of a group, which
+// run side by side and split the SMs) the score is the time weighted by the
+// fraction of the GPU the launch fills (bnm_integrator_share): SM time, not
+// latency.  A plan keeps the shape of its first tuning for a batch size,
+// whichever path ran it, so the same inputs give the same results through
+// bnm_run and through a group.  BNM_B200_SHAPE="kind,slots,csize,rpw,kr"
 // forces a shape; BNM_B200_SLOTS forces the register kernel's slots;
 // BNM_B200_TUNE=0 takes the first candidate untimed.
-static int tune_integrator(bnm_plan* p, const SimArgs& a) {
+static int tune_integrator(bnm_plan* p, const SimArgs& a, bool share = false) {
     const int n = a.n_sims;
     if (p->tuned_n == n) return BNM_OK;
     IntegratorShape cand[128];
@@ -483,8 +488,9 @@ static int tune_integrator(bnm_plan* p, const SimArgs& a) {
         if (!ok) continue;
         BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->tev[0], p->tev[1]));
         p->n_tried++;
-        if (ms < best) {
-            best = ms;
+        const double score = share ? ms * bnm_integrator_share(t, cand[i], p->num_sms) : ms;
+        if (score < best) {
+            best = score;
             p->shape = cand[i];
         }
     }
@@ -1120,7 +1126,7 @@ extern "C" int bnm_group_run(bnm_group* g, const int32_t* n, const double* const
                 BNM_CUDA_TRY(cudaMemcpy(p->d_wEE, p->io_wEE, (size_t)sizes[i] * p->cfg.nodes * 8, cudaMemcpyHostToDevice));
                 BNM_CUDA_TRY(cudaMemcpy(p->d_wEI, p->io_wEI, (size_t)sizes[i] * p->cfg.nodes * 8, cudaMemcpyHostToDevice));
                 if ((rc = launch_fic(p, sizes[i]))) return rc;
-                if ((rc = tune_integrator(p, sim_args(p, sizes[i])))) return rc;
+                if ((rc = tune_integrator(p, sim_args(p, sizes[i]), np > 1))) return rc;
             }
         }
         BNM_CUDA_TRY(cudaEventRecord(g->t0, g->origin));

@@ -487,6 +487,14 @@ extern "C" int bnm_cluster_probe(int N, int csize, int rpw, int kr, int n_sims, 
     return 0;
 }
 
+// Fraction of the GPU one launch of this shape fills: its clusters over the
+// clusters that can be resident at once (1 when the query fails).
+extern "C" double bnm_cluster_share(int N, int csize, int rpw, int kr, int n_sims) {
+    int out[6];
+    if (bnm_cluster_probe(N, csize, rpw, kr, n_sims, out) || out[5] < 1) return 1.0;
+    return n_sims >= out[5] ? 1.0 : (double)n_sims / out[5];
+}
+
 cudaError_t bnm_launch_integrate_cluster(const SimArgs& a, int csize, int rpw, int kr, cudaStream_t st) {
     int threads = 0, R = 0;
     size_t smem = 0;

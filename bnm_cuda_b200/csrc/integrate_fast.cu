@@ -370,6 +370,25 @@ static cudaError_t launch_fast(const SimArgs& a, int grid, cudaStream_t st) {
     return cudaGetLastError();
 }
 
+template <int K, int P>
+static double share_fast(const SimArgs& a, int grid, int num_sms) {
+    const int threads = ((a.N + 31) / 32) * 32;
+    const size_t smem = (size_t)P * kStages * 10 * a.N * sizeof(float2) + (size_t)a.N * 4 * K * sizeof(float) +
+                        (size_t)P * 2 * 4 * K * sizeof(float) + (size_t)P * 6 * threads * sizeof(double) +
+                        (1 + P * kStages) * sizeof(uint64_t);
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(integrate_fast_kernel<K, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, integrate_fast_kernel<K, P>, threads, smem) !=
+            cudaSuccess ||
+        per_sm < 1) {
+        cudaGetLastError();
+        return 1.0;
+    }
+    const double cap = (double)per_sm * num_sms;
+    return grid >= cap ? 1.0 : grid / cap;
+}
+
 }  // namespace bnm
 
 // Padded SC row length (4K) of the register kernel for a node count (0 = the
@@ -402,7 +421,8 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
         }
     }
     if (sh.kind == 1) return bnm_launch_integrate_cluster(a, sh.csize, sh.rpw, sh.kr, st);
-    if (sh.kind == 3) return bnm_launch_integrate_colsplit(a, sh.csize, sh.rpw, sh.slots, sh.kr, st);
+    if (sh.kind == 3 || sh.kind == 4)
+        return bnm_launch_integrate_colsplit(a, sh.csize, sh.rpw, sh.slots, sh.kr, sh.kind == 4 ? 2 : 1, st);
     if (sh.kind != 2) return cudaErrorInvalidValue;
     const int threads = ((a.N + 31) / 32) * 32;
     if (threads > 1024) return cudaErrorInvalidValue;
@@ -416,6 +436,30 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
     const int grid = a.n_sims < 2 * num_sms ? a.n_sims : 2 * num_sms;
     fastgen::integrate_generic_kernel<float><<<grid, threads, smem, st>>>(a, sc_in_smem);
     return cudaGetLastError();
+}
+
+double bnm_integrator_share(const bnm::SimArgs& a, const bnm::IntegratorShape& sh, int num_sms) {
+    using namespace bnm;
+    if (sh.kind == 0) {
+        const int ld = bnm_fast_kmax(a.N);
+        if (!ld || (sh.slots != 1 && sh.slots != 2)) return 1.0;
+        const int P = sh.slots;
+        int grid = (a.n_sims + P - 1) / P;
+        const int max_grid = P == 1 ? 2 * num_sms : num_sms;
+        if (grid > max_grid) grid = max_grid;
+        switch ((ld / 4) * 4 + P) {
+#define BNM_K(K)                                                  \
+    case K * 4 + 1: return share_fast<K, 1>(a, grid, num_sms); \
+    case K * 4 + 2: return share_fast<K, 2>(a, grid, num_sms);
+            BNM_K(4) BNM_K(8) BNM_K(12) BNM_K(16) BNM_K(20) BNM_K(24) BNM_K(28) BNM_K(32)
+#undef BNM_K
+            default: return 1.0;
+        }
+    }
+    if (sh.kind == 1) return bnm_cluster_share(a.N, sh.csize, sh.rpw, sh.kr, a.n_sims);
+    if (sh.kind == 3 || sh.kind == 4)
+        return bnm_colsplit_share(a.N, sh.csize, sh.rpw, sh.slots, sh.kr, sh.kind == 4 ? 2 : 1, a.n_sims);
+    return 1.0;  // the reference-order kernel fills the GPU (two CTAs per SM, persistent)
 }
 
 int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max) {
@@ -441,17 +485,18 @@ int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max) {
             if (bnm_cluster_shape(N, cs, shapes[v][0], shapes[v][1], &threads, &rows, &smem))
                 add({1, 0, cs, shapes[v][0], shapes[v][1]});
         }
-    int vs[3 * 64];
+    int vs[4 * 64];
     const int nv = bnm_colsplit_variants(vs, 64);
     for (int cs : {1, 2, 4, 8})
         for (int v = 0; v < nv && v < 64; v++) {
             int threads, rows;
             size_t smem;
-            const int rpl = vs[3 * v], k2 = vs[3 * v + 1], krp = vs[3 * v + 2];
+            const int rpl = vs[4 * v], k2 = vs[4 * v + 1], krp = vs[4 * v + 2], np = vs[4 * v + 3];
             bool dup = false;  // the variant table repeats (rpl, k2, k2) when k2 <= 8
             for (int u = 0; u < v; u++)
-                dup |= vs[3 * u] == rpl && vs[3 * u + 1] == k2 && vs[3 * u + 2] == krp;
-            if (!dup && bnm_colsplit_shape(N, cs, rpl, k2, krp, &threads, &rows, &smem)) add({3, k2, cs, rpl, krp});
+                dup |= vs[4 * u] == rpl && vs[4 * u + 1] == k2 && vs[4 * u + 2] == krp && vs[4 * u + 3] == np;
+            if (!dup && bnm_colsplit_shape(N, cs, rpl, k2, krp, np, &threads, &rows, &smem))
+                add({np == 2 ? 4 : 3, k2, cs, rpl, krp});
         }
     add({2, 0, 0, 0, 0});
     return n < max ? n : max;

@@ -152,19 +152,28 @@ namespace bnm {
 // column chunks in registers; kind 2: the reference-order kernel in FP32 (any
 // N); kind 3: column-split cluster kernel (N <= 512, even) with `csize` CTAs
 // per particle, `slots` column pairs per warp, `rpw` rows per lane and `kr`
-// column pairs in registers.
+// column pairs in registers; kind 4: column-split cluster kernel with two
+// particles per cluster (fields as kind 3).
 struct IntegratorShape {
     int kind, slots, csize, rpw, kr;
 };
 }  // namespace bnm
 cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::IntegratorShape& s, int num_sms,
                                        cudaStream_t st);
+// Fraction of the GPU (0, 1] one launch of shape s for a.n_sims particles
+// fills, by the kernel's own occupancy limit: the SM share a tuner weighs
+// when several plans run side by side.
+double bnm_integrator_share(const bnm::SimArgs& a, const bnm::IntegratorShape& s, int num_sms);
+extern "C" double bnm_cluster_share(int N, int csize, int rpw, int kr, int n_sims);
+extern "C" double bnm_colsplit_share(int N, int csize, int rpl, int k2, int krp, int np, int n_sims);
 // Candidate shapes for N nodes (those that compile to a launchable kernel); returns the count.
 int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max);
 cudaError_t bnm_launch_integrate_cluster(const bnm::SimArgs& a, int csize, int rpw, int kr, cudaStream_t st);
-cudaError_t bnm_launch_integrate_colsplit(const bnm::SimArgs& a, int csize, int rpl, int k2, int krp, cudaStream_t st);
-extern "C" int bnm_colsplit_shape(int N, int csize, int rpl, int k2, int krp, int* threads, int* rows, size_t* smem);
-extern "C" int bnm_colsplit_variants(int* out3, int max);
+cudaError_t bnm_launch_integrate_colsplit(const bnm::SimArgs& a, int csize, int rpl, int k2, int krp, int np,
+                                          cudaStream_t st);
+extern "C" int bnm_colsplit_shape(int N, int csize, int rpl, int k2, int krp, int np, int* threads, int* rows,
+                                  size_t* smem);
+extern "C" int bnm_colsplit_variants(int* out4, int max);
 extern "C" int bnm_cluster_shape(int N, int csize, int rpw, int kr, int* threads, int* rows, size_t* smem);
 cudaError_t bnm_launch_integrate_exact(const bnm::SimArgs& a, int fp64, int num_sms, cudaStream_t st);
 cudaError_t bnm_launch_fc_window(const bnm::FcArgs& a, cudaStream_t st);

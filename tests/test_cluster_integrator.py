@@ -5,8 +5,11 @@ mt19937 stream, bnm.cpp:38-43, fed to both).
 Every kind of cluster shape the autotuner can pick is forced once
 (BNM_B200_SHAPE): row-split (1, 2, 4 and 8 CTAs per particle, 8 or 16 nodes
 per warp) and column-split (2 to 7 rows per lane, 8 to 25 column pairs per
-warp, one-CTA clusters with a local S_E exchange included), with SC in
-registers only or split between registers and shared memory.  Bar, as for
+warp, one-CTA clusters with a local S_E exchange included, one or two
+particles per cluster), with SC in registers only or split between registers
+and shared memory.  Two particles per cluster restart together when either
+one's FIC check fails; the other's results must still be those of a run
+alone, which the per-particle comparison with the oracle checks.  Bar, as for
 the register kernel (N <= 128): on particles whose numerical FIC took the same
 decisions, BOLD within 1e-3 of its range, FC / FCD within 1e-3, cost within
 1e-2; wIE equal to the oracle's up to FP32 rounding.
@@ -27,15 +30,19 @@ SETUPS = {
     "n400": (400, 11000, 500, 2, 6, 2, 2, 2),
 }
 # kind,slots,csize,rpw,kr: kind 1 row-split (rpw nodes per warp, kr chunks in registers); kind 3
-# column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers)
+# column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers); kind 4
+# column-split with two particles per cluster
 SHAPES = {
     "n160": ["1,0,1,8,4", "1,0,2,8,5", "1,0,4,16,4", "1,0,8,8,4",
              "3,10,2,4,10", "3,8,4,2,8", "3,13,2,4,8",
              # one-CTA clusters: S_E exchanged through local shared memory
-             "3,10,1,5,10", "3,12,1,6,12", "3,13,1,7,13"],
-    "n400": ["1,0,4,8,4", "1,0,8,8,8", "1,0,8,16,4", "3,25,4,4,8", "3,13,8,2,13", "3,25,8,2,25"],
+             "3,10,1,5,10", "3,12,1,6,12", "3,13,1,7,13",
+             # two particles per cluster (three particles: one cluster's second half idles)
+             "4,10,2,4,10", "4,10,4,2,10"],
+    "n400": ["1,0,4,8,4", "1,0,8,8,8", "1,0,8,16,4", "3,25,4,4,8", "3,13,8,2,13", "3,25,8,2,25",
+             "4,25,4,4,25", "4,25,4,4,20", "4,13,8,2,13"],
 }
-KINDS = {1: "cluster", 3: "colsplit"}
+KINDS = {1: "cluster", 3: "colsplit", 4: "colsplit2"}
 
 
 @pytest.fixture(scope="module")
@@ -96,5 +103,5 @@ def test_autotuner_picks_a_timed_cluster_shape(cases):
         info = p.integrator()
         r2 = p.run(c["G"], c["wEE"], c["wEI"])  # tuned once per batch size
         assert p.integrator() == info
-    assert info["kind"] in ("cluster", "colsplit") and info["tried"] >= 4, info
+    assert info["kind"] in ("cluster", "colsplit", "colsplit2") and info["tried"] >= 4, info
     np.testing.assert_array_equal(r1["cost"], r2["cost"])

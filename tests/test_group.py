@@ -57,6 +57,26 @@ def test_group_graph_matches_per_plan_runs():
         p.close()
 
 
+def test_group_tunes_fresh_plans_for_sm_time():
+    """Plans first run through a group are tuned by SM time (the launch's time
+    weighted by the fraction of the GPU it fills), and keep that shape: a later
+    bnm_run of the same batch size gives the group's results exactly."""
+    plans, params = _subjects(6)
+    with B.Group(plans) as g:
+        first = g.run(params)
+        second = g.run(params)
+        for a, b in zip(first, second):
+            _same(a, b)
+    kinds = [p.integrator()["kind"] for p in plans]
+    assert kinds[:2] == ["register", "register"], kinds
+    assert kinds[2] in ("cluster", "colsplit", "colsplit2"), kinds
+    assert all(p.integrator()["tried"] >= 2 for p in plans)
+    for p, prm, r in zip(plans, params, first):
+        _same(p.run(*prm, outputs=("w_ie",)), r)
+    for p in plans:
+        p.close()
+
+
 def test_group_rejects_bad_inputs():
     plans, params = _subjects(3)
     with B.Group(plans) as g:
