@@ -191,12 +191,14 @@ int bnm_last_timings(bnm_plan *plan, double *ms6);
 /* FP32 integrator configuration the autotuner picked for the plan's last
  * batch size (no counterpart in the reference, which has one kernel shape).
  * out5: kind (0 register-SC kernel for N <= 128; 1 row-split and 3
- * column-split thread-block-cluster kernels for 128 < N <= 512; 2
- * reference-order kernel), then kind 0: particles per CTA; kind 1: -, CTAs
- * per particle, nodes per warp, SC column chunks of 32 in registers; kind 3:
- * column pairs per warp, CTAs per particle, rows per lane, column pairs in
- * registers.  *n_tried: candidate shapes timed.  The tuner runs on
- * the first bnm_run of each batch size; BNM_B200_SHAPE="k,s,c,r,kr" forces a
+ * column-split thread-block-cluster kernels for 128 < N <= 512, 4 the
+ * column-split kernel with two particles per cluster; 2 reference-order
+ * kernel), then kind 0: particles per CTA; kind 1: -, CTAs per particle,
+ * nodes per warp, SC column chunks of 32 in registers; kinds 3 and 4: column
+ * pairs per warp, CTAs per cluster, rows per lane, column pairs in
+ * registers.  *n_tried: candidate shapes timed.  The tuner runs on the first
+ * run of each batch size (by time for bnm_run, by SM time for the plans of a
+ * group) and the plan keeps that shape; BNM_B200_SHAPE="k,s,c,r,kr" forces a
  * shape and BNM_B200_TUNE=0 skips the timing. */
 int bnm_plan_integrator(bnm_plan *plan, int32_t *out5, int32_t *n_tried);
 
