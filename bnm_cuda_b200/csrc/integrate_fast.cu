@@ -4,13 +4,15 @@
 // CPU path (bnm.cpp:167-290), re-laid out for Blackwell:
 //   * one CTA per particle (persistent over particles, two CTAs per SM); warp
 //     w owns nodes 32w..32w+31.  The coupling G*J*(SC.S_E) is a register-
-//     blocked mat-vec: lane l = 4u+v of warp w keeps the 4 x K block
-//     SC[32w+4u .. 32w+4u+3][Kv .. Kv+K-1] in registers for the whole run,
-//     reads only its K entries of S_E (broadcast LDS.128), and the four lanes
+//     blocked mat-vec: lane l = 4u+v of warp w keeps the 4 x KC block
+//     SC[32w+4u .. 32w+4u+3][KC v .. KC v+KC-1] in registers for the whole
+//     run (KC = ceil(N/4) rounded up to even: 26 at N = 100), reads only its
+//     KC entries of S_E (broadcast LDS.128 from a buffer that keeps each
+//     quarter at a stride of K = KC rounded up to 4 floats), and the four lanes
 //     of a row group finish with a select-free 3-shuffle reduce-scatter (rows
 //     stored in xor-permuted slots) after which lane l holds the full sum of
 //     node 32w+l.  Shared-memory traffic per substep is
-//     K floats per lane instead of N;
+//     KC floats per lane instead of N;
 //   * SC is staged once into shared memory by a TMA bulk copy (cp.async.bulk
 //     + mbarrier, no multicast, bounded wait) before being read into registers;
 //   * the row dot products use packed FP32 FMA (fma.rn.f32x2) over column
@@ -59,11 +61,12 @@ struct Slot {
 // simulated millisecond per iteration in lockstep but keep their own time,
 // FIC trial and noise stream; a slot whose particle ends takes the next one
 // from the batch's work counter.
-template <int K, int P>
+template <int K, int KC, int P>
 __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     static_assert(K % 4 == 0 && K <= 32, "K");
+    static_assert(KC % 2 == 0 && KC <= K && KC + 2 >= K, "KC");
     static_assert(P >= 1 && P <= 2, "P");
-    constexpr int LD = 4 * K;  // padded SC row length and S_E buffer length
+    constexpr int LD = 4 * K;  // padded SC row length and S_E buffer length (quarter v at K v)
     typedef Model<float> C;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     // layout: [noise rings: P * kStages * 10*N float2][SC stage: N*LD floats]
@@ -81,6 +84,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     const int u = lane >> 2, v = lane & 3;
     const int j = threadIdx.x;  // node owned after the reduce-scatter (32w + lane)
     const bool act = j < N;
+    const int pos_j = K * (j / KC) + j % KC;  // S_E buffer slot of node j
     const long long kSpin = 1ll << 26;
 
     // ---- barriers; stage SC into shared memory with one TMA bulk copy ----
@@ -105,17 +109,17 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
         mbar_wait(smem_addr(mbar), 0, kSpin);  // let a late copy land before the CTA exits
         return;
     }
-    // This lane's 4 x K block of SC as column pairs.  Slot r of a lane holds
+    // This lane's 4 x KC block of SC as column pairs.  Slot r of a lane holds
     // row 4u + (v ^ r), so the reduce-scatter below keeps slot 0 and needs no
     // selects: after the xor-2 exchange slots 0 / 1 hold rows v / v^1, after
     // the xor-1 exchange slot 0 holds the full sum of row 4u + v.
-    float2 sc[4][K / 2];
+    float2 sc[4][KC / 2];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
         const int row = 32 * w + 4 * u + (v ^ r);
 #pragma unroll
-        for (int c = 0; c < K / 2; c++)
-            sc[r][c] = row < N ? reinterpret_cast<const float2*>(sc_stage + (size_t)row * LD + v * K)[c]
+        for (int c = 0; c < KC / 2; c++)
+            sc[r][c] = row < N ? reinterpret_cast<const float2*>(sc_stage + (size_t)row * LD + v * KC)[c]
                                : make_float2(0.f, 0.f);
     }
 
@@ -170,7 +174,10 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
         q.bw = BW();
 #pragma unroll
         for (int e = 0; e < 6; e++) ext[((size_t)p * 6 + e) * blockDim.x + threadIdx.x] = 0.0;
-        for (int k = threadIdx.x; k < 2 * LD; k += blockDim.x) S_buf[p * 2 * LD + k] = ((k % LD) < N) ? 0.001f : 0.f;
+        for (int k = threadIdx.x; k < 2 * LD; k += blockDim.x) {
+            const int o = (k % LD) % K, col = (k % LD) / K * KC + o;  // S_E slot -> column
+            S_buf[p * 2 * LD + k] = (o < KC && col < N) ? 0.001f : 0.f;
+        }
         ts[p] = 0;
         frame[p] = 0;
         to_frame[p] = 1;
@@ -217,7 +224,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
 #pragma unroll
                 for (int r = 0; r < 4; r++) acc[p][r] = make_float2(0.f, 0.f);
 #pragma unroll
-            for (int c4 = 0; c4 < K / 4; c4++) {
+            for (int c4 = 0; c4 < K / 4; c4++) {  // pairs 2 c4, 2 c4 + 1 (those below KC / 2)
 #pragma unroll
                 for (int p = 0; p < P; p++) {
                     const float4 s = reinterpret_cast<const float4*>(S_buf + (p * 2 + cur) * LD + v * K)[c4];
@@ -225,7 +232,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
 #pragma unroll
                     for (int r = 0; r < 4; r++) {
                         acc[p][r] = __ffma2_rn(sc[r][2 * c4], s01, acc[p][r]);
-                        acc[p][r] = __ffma2_rn(sc[r][2 * c4 + 1], s23, acc[p][r]);
+                        if (2 * c4 + 1 < KC / 2) acc[p][r] = __ffma2_rn(sc[r][2 * c4 + 1 < KC / 2 ? 2 * c4 + 1 : 0], s23, acc[p][r]);
                     }
                 }
             }
@@ -250,7 +257,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
                 const float dSI = fmaf(kDtGammaI, q.rI, fmaf(-kDtInvTauI, q.S_I, SQ * n.y));
                 q.S_E = __saturatef(q.S_E + dSE);
                 q.S_I = __saturatef(q.S_I + dSI);
-                if (act) S_buf[(p * 2 + (cur ^ 1)) * LD + j] = q.S_E;
+                if (act) S_buf[(p * 2 + (cur ^ 1)) * LD + pos_j] = q.S_E;
             }
             __syncthreads();
             cur ^= 1;
@@ -304,7 +311,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
                             q.mean_IE = 0.0;
 #pragma unroll
                             for (int e = 0; e < 6; e++) ext[((size_t)p * 6 + e) * blockDim.x + threadIdx.x] = 0.0;
-                            if (act) S_buf[(p * 2 + cur) * LD + j] = q.S_E;
+                            if (act) S_buf[(p * 2 + cur) * LD + pos_j] = q.S_E;
                             ts[p] = 0;
                             frame[p] = 0;
                             to_frame[p] = 1;
@@ -357,29 +364,29 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     }
 }
 
-template <int K, int P>
+template <int K, int KC, int P>
 static cudaError_t launch_fast(const SimArgs& a, int grid, cudaStream_t st) {
     const int threads = ((a.N + 31) / 32) * 32;
     const size_t smem = (size_t)P * kStages * 10 * a.N * sizeof(float2) + (size_t)a.N * 4 * K * sizeof(float) +
                         (size_t)P * 2 * 4 * K * sizeof(float) + (size_t)P * 6 * threads * sizeof(double) +
                         (1 + P * kStages) * sizeof(uint64_t);
     cudaError_t e =
-        cudaFuncSetAttribute(integrate_fast_kernel<K, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(integrate_fast_kernel<K, KC, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    integrate_fast_kernel<K, P><<<grid, threads, smem, st>>>(a);
+    integrate_fast_kernel<K, KC, P><<<grid, threads, smem, st>>>(a);
     return cudaGetLastError();
 }
 
-template <int K, int P>
+template <int K, int KC, int P>
 static double share_fast(const SimArgs& a, int grid, int num_sms) {
     const int threads = ((a.N + 31) / 32) * 32;
     const size_t smem = (size_t)P * kStages * 10 * a.N * sizeof(float2) + (size_t)a.N * 4 * K * sizeof(float) +
                         (size_t)P * 2 * 4 * K * sizeof(float) + (size_t)P * 6 * threads * sizeof(double) +
                         (1 + P * kStages) * sizeof(uint64_t);
     int per_sm = 0;
-    if (cudaFuncSetAttribute(integrate_fast_kernel<K, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, integrate_fast_kernel<K, P>, threads, smem) !=
+    if (cudaFuncSetAttribute(integrate_fast_kernel<K, KC, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, integrate_fast_kernel<K, KC, P>, threads, smem) !=
             cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
@@ -390,6 +397,9 @@ static double share_fast(const SimArgs& a, int grid, int num_sms) {
 }
 
 }  // namespace bnm
+
+// Columns per lane of the register kernel: ceil(N / 4) rounded up to even.
+static int fast_kc(int N) { return ((N + 3) / 4 + 1) / 2 * 2; }
 
 // Padded SC row length (4K) of the register kernel for a node count (0 = the
 // register kernel does not cover it).
@@ -411,10 +421,13 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
         int grid = (a.n_sims + P - 1) / P;
         const int max_grid = P == 1 ? 2 * num_sms : num_sms;
         if (grid > max_grid) grid = max_grid;
-        switch ((ld / 4) * 4 + P) {
-#define BNM_K(K)                                          \
-    case K * 4 + 1: return launch_fast<K, 1>(a, grid, st); \
-    case K * 4 + 2: return launch_fast<K, 2>(a, grid, st);
+        const int kc = fast_kc(a.N);
+        switch ((ld / 4) * 8 + (ld / 4 - kc) * 2 + P) {
+#define BNM_K(K)                                                            \
+    case K * 8 + 1: return launch_fast<K, K, 1>(a, grid, st);            \
+    case K * 8 + 2: return launch_fast<K, K, 2>(a, grid, st);            \
+    case K * 8 + 4 + 1: return launch_fast<K, K - 2, 1>(a, grid, st); \
+    case K * 8 + 4 + 2: return launch_fast<K, K - 2, 2>(a, grid, st);
             BNM_K(4) BNM_K(8) BNM_K(12) BNM_K(16) BNM_K(20) BNM_K(24) BNM_K(28) BNM_K(32)
 #undef BNM_K
             default: return cudaErrorInvalidValue;
@@ -447,10 +460,13 @@ double bnm_integrator_share(const bnm::SimArgs& a, const bnm::IntegratorShape& s
         int grid = (a.n_sims + P - 1) / P;
         const int max_grid = P == 1 ? 2 * num_sms : num_sms;
         if (grid > max_grid) grid = max_grid;
-        switch ((ld / 4) * 4 + P) {
-#define BNM_K(K)                                                  \
-    case K * 4 + 1: return share_fast<K, 1>(a, grid, num_sms); \
-    case K * 4 + 2: return share_fast<K, 2>(a, grid, num_sms);
+        const int kc = fast_kc(a.N);
+        switch ((ld / 4) * 8 + (ld / 4 - kc) * 2 + P) {
+#define BNM_K(K)                                                                  \
+    case K * 8 + 1: return share_fast<K, K, 1>(a, grid, num_sms);              \
+    case K * 8 + 2: return share_fast<K, K, 2>(a, grid, num_sms);              \
+    case K * 8 + 4 + 1: return share_fast<K, K - 2, 1>(a, grid, num_sms); \
+    case K * 8 + 4 + 2: return share_fast<K, K - 2, 2>(a, grid, num_sms);
             BNM_K(4) BNM_K(8) BNM_K(12) BNM_K(16) BNM_K(20) BNM_K(24) BNM_K(28) BNM_K(32)
 #undef BNM_K
             default: return 1.0;

@@ -1,17 +1,19 @@
-"""The thread-block-cluster FP32 integrator (128 < N <= 512) against the FP64
-oracle port, through the C ABI, in oracle-noise mode (the reference's
-mt19937 stream, bnm.cpp:38-43, fed to both).
+"""FP32 integrator shapes against the FP64 oracle port, through the C ABI, in
+oracle-noise mode (the reference's mt19937 stream, bnm.cpp:38-43, fed to
+both).
 
-Every kind of cluster shape the autotuner can pick is forced once
-(BNM_B200_SHAPE): row-split (1, 2, 4 and 8 CTAs per particle, 8 or 16 nodes
-per warp) and column-split (2 to 7 rows per lane, 8 to 25 column pairs per
+Every kind of shape the autotuner can pick is forced once (BNM_B200_SHAPE):
+the register-SC kernel (N <= 128) at N = 68 and 100, where each lane's SC
+block is narrower than its 16-byte-aligned S_E stride (18 of 20 and 26 of 28
+columns), with one and two particles per CTA; and for 128 < N <= 512 the
+thread-block-cluster kernels, row-split (1, 2, 4 and 8 CTAs per particle, 8
+or 16 nodes per warp) and column-split (2 to 7 rows per lane, 8 to 25 column pairs per
 warp, one-CTA clusters with a local S_E exchange included, one or two
 particles per cluster), with SC in registers only or split between registers
 and shared memory.  Two particles per cluster restart together when either
 one's FIC check fails; the other's results must still be those of a run
-alone, which the per-particle comparison with the oracle checks.  Bar, as for
-the register kernel (N <= 128): on particles whose numerical FIC took the same
-decisions, BOLD within 1e-3 of its range, FC / FCD within 1e-3, cost within
+alone, which the per-particle comparison with the oracle checks.  Bar: on
+particles whose numerical FIC took the same decisions, BOLD within 1e-3 of its range, FC / FCD within 1e-3, cost within
 1e-2; wIE equal to the oracle's up to FP32 rounding.
 """
 import concurrent.futures as cf
@@ -26,13 +28,17 @@ pytestmark = pytest.mark.gpu
 
 # N, T ms, TR, remove s, window, step, max trials, particles
 SETUPS = {
+    "n68": (68, 12000, 500, 2, 6, 2, 3, 3),
+    "n100": (100, 15000, 500, 2, 10, 2, 10, 3),
     "n160": (160, 15000, 500, 2, 10, 2, 10, 3),
     "n400": (400, 11000, 500, 2, 6, 2, 2, 2),
 }
-# kind,slots,csize,rpw,kr: kind 1 row-split (rpw nodes per warp, kr chunks in registers); kind 3
+# kind,slots,csize,rpw,kr: kind 0 register-SC (slots particles per CTA); kind 1 row-split (rpw nodes per warp, kr chunks in registers); kind 3
 # column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers); kind 4
 # column-split with two particles per cluster
 SHAPES = {
+    "n68": ["0,1,0,0,0", "0,2,0,0,0"],
+    "n100": ["0,1,0,0,0", "0,2,0,0,0"],
     "n160": ["1,0,1,8,4", "1,0,2,8,5", "1,0,4,16,4", "1,0,8,8,4",
              "3,10,2,4,10", "3,8,4,2,8", "3,13,2,4,8",
              # one-CTA clusters: S_E exchanged through local shared memory
@@ -42,7 +48,7 @@ SHAPES = {
     "n400": ["1,0,4,8,4", "1,0,8,8,8", "1,0,8,16,4", "3,25,4,4,8", "3,13,8,2,13", "3,25,8,2,25",
              "4,25,4,4,25", "4,25,4,4,20", "4,13,8,2,13"],
 }
-KINDS = {1: "cluster", 3: "colsplit", 4: "colsplit2"}
+KINDS = {0: "register", 1: "cluster", 3: "colsplit", 4: "colsplit2"}
 
 
 @pytest.fixture(scope="module")
