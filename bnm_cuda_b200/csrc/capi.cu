@@ -470,6 +470,8 @@ static int tune_integrator(bnm_plan* p, const SimArgs& a, bool share = false) {
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, p->st));
     double best = 1e300;
     for (int i = 0; i < nc; i++) {
+        // shapes that integrate two particles together compute an idle one for a batch of one
+        if (n < 2 && ((cand[i].kind == 0 && cand[i].slots == 2) || cand[i].kind == 4)) continue;
         float ms = 0.f;
         bool ok = true;
         for (int rep = 0; rep < 2 && ok; rep++) {  // the first launch also loads the kernel
