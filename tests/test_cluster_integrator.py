@@ -3,9 +3,10 @@ oracle-noise mode (the reference's mt19937 stream, bnm.cpp:38-43, fed to
 both).
 
 Every kind of shape the autotuner can pick is forced once (BNM_B200_SHAPE):
-the register-SC kernel (N <= 128) at N = 68 and 100, where each lane's SC
-block is narrower than its 16-byte-aligned S_E stride (18 of 20 and 26 of 28
-columns), with one and two particles per CTA; and for 128 < N <= 512 the
+the register-SC kernel (N <= 128) at N = 67, 68 and 100, where each lane's SC
+block is narrower than its 16-byte-aligned S_E stride (18 of 20, 18 of 20 and
+26 of 28 columns; N = 67 with a partly filled last warp), and at N = 128 with
+full 32-column blocks, with one and two particles per CTA; and for 128 < N <= 512 the
 thread-block-cluster kernels, row-split (1, 2, 4 and 8 CTAs per particle, 8
 or 16 nodes per warp) and column-split (2 to 7 rows per lane, 8 to 25 column pairs per
 warp, one-CTA clusters with a local S_E exchange included, one or two
@@ -28,8 +29,10 @@ pytestmark = pytest.mark.gpu
 
 # N, T ms, TR, remove s, window, step, max trials, particles
 SETUPS = {
+    "n67": (67, 11000, 500, 2, 6, 2, 3, 3),
     "n68": (68, 12000, 500, 2, 6, 2, 3, 3),
     "n100": (100, 15000, 500, 2, 10, 2, 10, 3),
+    "n128": (128, 11000, 500, 2, 6, 2, 3, 2),
     "n160": (160, 15000, 500, 2, 10, 2, 10, 3),
     "n400": (400, 11000, 500, 2, 6, 2, 2, 2),
 }
@@ -37,8 +40,10 @@ SETUPS = {
 # column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers); kind 4
 # column-split with two particles per cluster
 SHAPES = {
+    "n67": ["0,1,0,0,0"],
     "n68": ["0,1,0,0,0", "0,2,0,0,0"],
     "n100": ["0,1,0,0,0", "0,2,0,0,0"],
+    "n128": ["0,1,0,0,0"],
     "n160": ["1,0,1,8,4", "1,0,2,8,5", "1,0,4,16,4", "1,0,8,8,4",
              "3,10,2,4,10", "3,8,4,2,8", "3,13,2,4,8",
              # one-CTA clusters: S_E exchanged through local shared memory
@@ -55,10 +60,11 @@ KINDS = {0: "register", 1: "cluster", 3: "colsplit", 4: "colsplit2"}
 def cases(port):
     out = {}
     for name, (N, T, TR, remove, ws, step, trials, n) in SETUPS.items():
+        exc = N % 2 == 0  # the hemisphere split (exc_interhem) needs an even node count
         sc = synth.make_sc(N, 0.3 if N < 300 else 0.1, 7)
         G, wEE, wEI = synth.uniform_params(n, N, seed=21, g=(0.5, 2.0))
         cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TR, window_size=ws, window_step=step,
-                       bold_remove_s=remove, exc_interhem=True, max_fic_trials=trials, noise_mode=B.NOISE_HOST)
+                       bold_remove_s=remove, exc_interhem=exc, max_fic_trials=trials, noise_mode=B.NOISE_HOST)
         s = cfg.sizes()
         noise = port.port_noise(410, s["noise_len"])
         wie0 = np.stack([port.port_analytic_fic(sc, G[i], wEE[i], wEI[i])[0] for i in range(n)])
@@ -71,11 +77,11 @@ def cases(port):
             ref = list(ex.map(one, range(n)))
         bold = np.stack([r["bold"] for r in ref])
         kept = bold[:, s["n_vols_remove"]:]
-        fc = np.stack([port.port_fc_tril(k) for k in kept])
-        fcd = np.stack([port.port_fcd_tril(k, step, ws) for k in kept])
+        fc = np.stack([port.port_fc_tril(k, exc) for k in kept])
+        fcd = np.stack([port.port_fcd_tril(k, step, ws, exc) for k in kept])
         rng = np.random.default_rng(5)
         emp_fc, emp_fcd = rng.uniform(-0.2, 0.8, fc.shape[1]), rng.uniform(-0.3, 1.0, 500)
-        cost = np.array([port.port_gof(k, step, ws, emp_fc, emp_fcd)["cost"] for k in kept])
+        cost = np.array([port.port_gof(k, step, ws, emp_fc, emp_fcd, exc)["cost"] for k in kept])
         out[name] = dict(cfg=cfg, sc=sc, G=G, wEE=wEE, wEI=wEI, wie0=wie0, noise=noise, bold=bold, fc=fc, fcd=fcd,
                          cost=cost, emp_fc=emp_fc, emp_fcd=emp_fcd, trials=np.array([r["trials"] for r in ref]),
                          wIE=np.stack([r["wIE"] for r in ref]))
