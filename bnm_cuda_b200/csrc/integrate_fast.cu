@@ -9,9 +9,9 @@
 //     run (KC = ceil(N/4) rounded up to even: 26 at N = 100), reads only its
 //     KC entries of S_E (broadcast LDS.128 from a buffer that keeps each
 //     quarter at a stride of K = KC rounded up to 4 floats), and the four lanes
-//     of a row group finish with a select-free 3-shuffle reduce-scatter (rows
-//     stored in xor-permuted slots) after which lane l holds the full sum of
-//     node 32w+l.  Shared-memory traffic per substep is
+//     of a row group finish with a select-free reduce-scatter of three
+//     independent shuffles (rows stored in xor-permuted slots) after which
+//     lane l holds the full sum of node 32w+l.  Shared-memory traffic per substep is
 //     KC floats per lane instead of N;
 //   * SC is staged once into shared memory by a TMA bulk copy (cp.async.bulk
 //     + mbarrier, no multicast, bounded wait) before being read into registers;
@@ -110,9 +110,9 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
         return;
     }
     // This lane's 4 x KC block of SC as column pairs.  Slot r of a lane holds
-    // row 4u + (v ^ r), so the reduce-scatter below keeps slot 0 and needs no
-    // selects: after the xor-2 exchange slots 0 / 1 hold rows v / v^1, after
-    // the xor-1 exchange slot 0 holds the full sum of row 4u + v.
+    // row 4u + (v ^ r), so the reduce-scatter below needs no selects: lane v
+    // adds its slot 0 and slot m of lane v ^ m (m = 1, 2, 3), all of them row
+    // 4u + v.
     float2 sc[4][KC / 2];
 #pragma unroll
     for (int r = 0; r < 4; r++) {
@@ -239,12 +239,13 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
 #pragma unroll
             for (int p = 0; p < P; p++) {
                 Slot& q = sl[p];
-                // reduce-scatter over the 4 lanes of this row group (see the SC slot order)
-                const float q0 =
-                    (acc[p][0].x + acc[p][0].y) + __shfl_xor_sync(0xffffffffu, acc[p][2].x + acc[p][2].y, 2);
-                const float q1 =
-                    (acc[p][1].x + acc[p][1].y) + __shfl_xor_sync(0xffffffffu, acc[p][3].x + acc[p][3].y, 2);
-                const float coupling = q0 + __shfl_xor_sync(0xffffffffu, q1, 1);
+                // reduce-scatter over the 4 lanes of this row group: lane v ^ m keeps
+                // row v in its slot m, so the three exchanges are independent (one
+                // shuffle latency on the chain instead of two)
+                const float r1 = __shfl_xor_sync(0xffffffffu, acc[p][1].x + acc[p][1].y, 1);
+                const float r2 = __shfl_xor_sync(0xffffffffu, acc[p][2].x + acc[p][2].y, 2);
+                const float r3 = __shfl_xor_sync(0xffffffffu, acc[p][3].x + acc[p][3].y, 3);
+                const float coupling = ((acc[p][0].x + acc[p][0].y) + r1) + (r2 + r3);
                 const float2 n = act ? nz[p][(size_t)sub * N] : make_float2(0.f, 0.f);
                 q.IE = fmaf(q.GJ, coupling, fmaf(q.wEE, q.S_E, C::w_E__I_0)) - q.wIE * q.S_I;
                 q.II = fmaf(q.wEI, q.S_E, C::w_I__I_0) - q.S_I;
