@@ -137,13 +137,14 @@ class _QuietStdout:
 _TRIALS = {}
 
 
-def cpu_reference_sample(n_threads: int, sample_ms: int = SAMPLE_MS):
+def cpu_reference_sample(n_threads: int, sample_ms: int = SAMPLE_MS, fp32: bool = False):
     """One bounded sample of the reference's CPU run_simulations (see module
-    docstring).  Returns (sims_per_s, detail)."""
+    docstring); fp32 times the reference's -DUSE_FLOATS build instead of its
+    default double build.  Returns (sims_per_s, detail)."""
     os.environ.setdefault("OMP_NUM_THREADS", str(n_threads))
     from oracle import ref
 
-    if not ref.ref_available():
+    if not ref.ref_available(fp32):
         return None
     sc, G, wEE, wEI = workload_inputs(1)
     idx = np.arange(n_threads) % N_SIMS
@@ -155,20 +156,20 @@ def cpu_reference_sample(n_threads: int, sample_ms: int = SAMPLE_MS):
         t0 = time.perf_counter()
         ref.ref_run_simulations(sc, G[idx], wEE[idx], wEI[idx], zeros if fic else zeros + 1.0, time_steps=sample_ms,
                                 bold_tr=1000, rand_seed=410, max_fic_trials=10, emp_fc=emp_fc, emp_fcd=emp_fcd,
-                                window_step=1, window_size=2, sim_only=True)
+                                window_step=1, window_size=2, sim_only=True, fp32=fp32)
         t_sample = time.perf_counter() - t0
     if not fic:
         return None
     # FIC restarts of these particles (they happen in the first 10 s).  The
     # reference only reports them in its text output; the port reproduces the
     # reference bit for bit, so the counts come from it, once per process.
-    key = (n_threads,)
+    key = (n_threads, fp32)
     if key not in _TRIALS:
         with _QuietStdout():
             _TRIALS[key] = ref.port_run_batch(
                 sc, G[idx], wEE[idx], wEI[idx], zeros, time_steps=10_000, bold_tr=1000, n_vols_remove=0, seed=410,
                 window_step=1, window_size=2, emp_fc=np.zeros(20), emp_fcd=np.zeros(10),
-                n_threads=n_threads)["trials"] if ref.port_available() else np.zeros(n)
+                n_threads=n_threads, fp32=fp32)["trials"] if ref.port_available() else np.zeros(n)
     tr = _TRIALS[key]
     s_sample = 10 * (sample_ms + 1) + 100_000 * tr
     s_full = 10 * (T_MS + 1) + 100_000 * tr
@@ -178,7 +179,7 @@ def cpu_reference_sample(n_threads: int, sample_ms: int = SAMPLE_MS):
     t1 = time.perf_counter()
     with _QuietStdout():
         ref.ref_check_fit_bold(bold, STEP, WS, np.random.default_rng(2).uniform(-1, 1, 2450),
-                               np.random.default_rng(1).uniform(-1, 1, 1000))
+                               np.random.default_rng(1).uniform(-1, 1, 1000), fp32=fp32)
     t_gof = time.perf_counter() - t1
     per_sim = s_full.mean() / rate + t_gof
     sims_per_s = n_threads / per_sim
@@ -283,7 +284,9 @@ def run_b200(args):
     if rank == 0:
         peak = B.measure_fp32_peak(local)
         achieved = float(np.mean(np.array(flops) / (np.array(integ_ms) * 1e-3))) / 1e12
-        cpu = cpu_reference_sample(len(os.sched_getaffinity(0))) if (world == 1 and not args.no_cpu) else None
+        cores = len(os.sched_getaffinity(0))
+        cpu = cpu_reference_sample(cores) if (world == 1 and not args.no_cpu) else None
+        cpu32 = cpu_reference_sample(cores, fp32=True) if (world == 1 and not args.no_cpu) else None
         n, N = N_SIMS, N_NODES
         result = {
             "metric": "sims/s", "value": value, "unit": "sims/s", "n_gpus": world, "steps": args.steps,
@@ -309,8 +312,11 @@ def run_b200(args):
             "clocks": clk.summary(),
         }
         if cpu is not None:
-            result["cpu_baseline"] = {"value": cpu[0], "unit": "sims/s", "cores": len(os.sched_getaffinity(0)),
+            result["cpu_baseline"] = {"value": cpu[0], "unit": "sims/s", "cores": cores,
                                       "kind": "reference", "sample": cpu[1]["sample"]}
+        if cpu32 is not None:  # the reference's float build (-DUSE_FLOATS), same sample
+            result["cpu_baseline_f32"] = {"value": cpu32[0], "unit": "sims/s", "cores": cores,
+                                          "kind": "reference", "sample": cpu32[1]["sample"]}
     plan.close()
     if dist:
         dist.barrier()

@@ -27,7 +27,7 @@ LIB_PATH = os.path.join(HERE, "libbnm_b200.so")
 BNM_OK, BNM_EINVAL, BNM_ENOMEM, BNM_ECUDA, BNM_ETIMEOUT = 0, 1, 2, 3, 4
 PREC_F32, PREC_F64, PREC_F32_REF = 0, 1, 2
 NOISE_PHILOX, NOISE_HOST = 0, 1
-GRAM_F32, GRAM_BF16, GRAM_BF16_SPLIT = 0, 1, 2
+GRAM_AUTO, GRAM_F32, GRAM_BF16, GRAM_BF16_SPLIT = -1, 0, 1, 2
 
 _lib = None
 
@@ -152,7 +152,7 @@ class Config:
     noise_mode: int = NOISE_PHILOX
     noise_seed: int = 410
     device: int = 0
-    gram: int = GRAM_BF16_SPLIT
+    gram: int = GRAM_AUTO  # split BF16 for PREC_F32, FP32 SIMT for the reference-order precisions
 
     @classmethod
     def from_env(cls, **overrides) -> "Config":

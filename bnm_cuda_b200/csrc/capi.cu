@@ -72,7 +72,7 @@ extern "C" void bnm_config_default(bnm_config* c) {
     c->noise_mode = BNM_NOISE_PHILOX;
     c->noise_seed = 410;
     c->device = 0;
-    c->gram = BNM_GRAM_BF16_SPLIT;
+    c->gram = BNM_GRAM_AUTO;
 }
 
 // helpers.cpp:4-19: ints through atoi; doubles through atof, returned as float.
@@ -219,7 +219,11 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
         return fail(BNM_EINVAL, "host noise needs %lld values (got %lld)", (long long)s.noise_len,
                     (long long)n_host_noise);
     if (cfg->precision < 0 || cfg->precision > 2) return fail(BNM_EINVAL, "unknown precision %d", cfg->precision);
-    if (cfg->gram < 0 || cfg->gram > 2) return fail(BNM_EINVAL, "unknown gram arithmetic %d", cfg->gram);
+    if (cfg->gram < BNM_GRAM_AUTO || cfg->gram > 2) return fail(BNM_EINVAL, "unknown gram arithmetic %d", cfg->gram);
+    // AUTO: tensor-core split BF16 for the FP32 product path, the FP32 / FP64
+    // SIMT analysis for the reference-order precisions
+    if (p->cfg.gram == BNM_GRAM_AUTO)
+        p->cfg.gram = cfg->precision == BNM_PREC_F32 ? BNM_GRAM_BF16_SPLIT : BNM_GRAM_F32;
     for (int i = 0; i < N * N; i++)
         if (!std::isfinite(sc[i])) return fail(BNM_EINVAL, "SC has a non-finite entry at %d", i);
 
@@ -325,8 +329,8 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
     BNM_CUDA_TRY(dalloc(p, &p->d_fcc, n));
     BNM_CUDA_TRY(dalloc(p, &p->d_fcdiff, n));
     BNM_CUDA_TRY(dalloc(p, &p->d_ks, n));
-    if (cfg->gram != BNM_GRAM_F32) {
-        const int parts = cfg->gram == BNM_GRAM_BF16_SPLIT ? 2 : 1;
+    if (p->cfg.gram != BNM_GRAM_F32) {
+        const int parts = p->cfg.gram == BNM_GRAM_BF16_SPLIT ? 2 : 1;
         auto blocks = [](int64_t x, int b) { return (int)((x + b - 1) / b); };
         p->fc_rb = blocks(N, kGramTileRows);
         p->fc_kb = blocks(s.corr_len, kGramTileK);

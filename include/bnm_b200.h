@@ -49,7 +49,7 @@ enum { BNM_NOISE_PHILOX = 0, BNM_NOISE_HOST = 1 };
  * BF16_SPLIT: FC and FCD as tcgen05 tensor-core Grams with FP32 accumulation,
  * operands rounded once to BF16, or split into hi + lo BF16 parts with the
  * hi.hi + hi.lo + lo.hi products accumulated (error near FP32's). */
-enum { BNM_GRAM_F32 = 0, BNM_GRAM_BF16 = 1, BNM_GRAM_BF16_SPLIT = 2 };
+enum { BNM_GRAM_AUTO = -1, BNM_GRAM_F32 = 0, BNM_GRAM_BF16 = 1, BNM_GRAM_BF16_SPLIT = 2 };
 
 /* Run configuration: the reference's CLI arguments and BNM_* settings. */
 typedef struct bnm_config {
@@ -77,7 +77,9 @@ typedef struct bnm_config {
     int32_t noise_mode;        /* BNM_NOISE_* */
     uint64_t noise_seed;       /* argv[16] */
     int32_t device;
-    int32_t gram;              /* BNM_GRAM_* (default BF16_SPLIT; no counterpart in the reference, which
+    int32_t gram;              /* BNM_GRAM_* (default AUTO: BF16_SPLIT for BNM_PREC_F32, F32 for the
+                                  reference-order precisions, whose results are compared with the
+                                  reference's own arithmetic; no counterpart in the reference, which
                                   runs FP32/FP64 SIMT) */
 } bnm_config;
 
