@@ -16,13 +16,14 @@
 //     table; after one barrier thread t < R adds the W partials of row t and
 //     updates node r0 + t alone (the row-split layout updates each node in
 //     32/RPW lanes);
-//   * two CTA barriers per substep: one after the S_E wait (all threads are
-//     past it before the buffer's next phase is armed, and the partial table
-//     of the previous substep has been read), one between partials and sums;
+//   * one CTA barrier per substep, between partials and sums: each thread
+//     waits for the S_E buffer on its mbarrier itself and the partial table
+//     alternates with the substep, so nothing else needs the whole block;
 //   * a cluster of one CTA (N up to 32 RPL, all of SC in registers) skips the
 //     asynchronous exchange: owners store S_E straight into the other buffer
-//     and the first barrier of the next substep orders it (the buffer being
-//     written was last read before that barrier of the previous substep).
+//     and a second barrier at the start of the next substep orders it (the
+//     buffer being written was last read before the partial-table barrier of
+//     the previous substep).
 #include <cstdlib>
 #include <cstring>
 #include <vector>
@@ -45,7 +46,7 @@ constexpr int kAgreeMs = 16;
 
 // Shared-memory layout (bytes), in this order:
 //   S      [2][P][2 K2 W] float          S_E of every node, double buffered, per particle
-//   red    [P][W][32 RPL] float          per-warp partial row sums
+//   red    [2][P][W][32 RPL] float       per-warp partial row sums, by substep parity
 //   SCs    [W][RPL][K2-KRP][32] float2   shared-memory part of the SC slice
 //   ring   [kRing][10][R] float2         noise of the own nodes, per millisecond
 //   ext    [P][6][32 RPL] double         extended-output sums of the own nodes
@@ -55,7 +56,7 @@ template <int RPL, int K2, int KRP, int P>
 struct ColLayout {
     static constexpr int kRP = 32 * RPL;
     __host__ __device__ static size_t red_off(int W) { return (size_t)2 * P * W * 2 * K2 * sizeof(float); }
-    __host__ __device__ static size_t sc_off(int W) { return red_off(W) + (size_t)P * W * kRP * sizeof(float); }
+    __host__ __device__ static size_t sc_off(int W) { return red_off(W) + (size_t)2 * P * W * kRP * sizeof(float); }
     __host__ __device__ static size_t ring_off(int W) {
         return sc_off(W) + (size_t)W * RPL * (K2 - KRP) * 32 * sizeof(float2);
     }
@@ -249,9 +250,16 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
         for (int sub = 0; sub < 10; sub++) {
             if (!solo && !skip_wait && !late) late = !wait_s(cur);
             skip_wait = false;
-            // all threads are past this phase (arm the buffer's next one), and
-            // the partial table of the previous substep has been read
-            __syncthreads();
+            // A one-CTA cluster stored S_E locally: a block barrier orders those
+            // stores before the reads below.  A cluster of several CTAs needs
+            // none here: every thread waited on buffer cur's mbarrier itself;
+            // the next phase of that buffer (S_E two substeps on) cannot
+            // complete, nor land in the buffer, before the other CTAs have this
+            // CTA's next S_E, which is sent after the block barrier below, when
+            // every thread has read buffer cur and passed this wait; and the
+            // partial table alternates with the substep, so this substep's
+            // partials never overwrite ones a slower thread is still adding.
+            if (solo) __syncthreads();
             if (!solo && t == 0 && !late)
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar_local + 8u * cur),
                              "r"(4 * N * P)
@@ -278,10 +286,11 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
 #pragma unroll
             for (int p = 0; p < P; p++)
 #pragma unroll
-                for (int i = 0; i < RPL; i++) red[(p * W + w) * RP + lane + 32 * i] = acc[p][i].x + acc[p][i].y;
+                for (int i = 0; i < RPL; i++)
+                    red[((cur * P + p) * W + w) * RP + lane + 32 * i] = acc[p][i].x + acc[p][i].y;
             __syncthreads();
             if ((tu >> 5) < upd_warps) {
-                const float* rp = red + slot * W * RP + tu;
+                const float* rp = red + (cur * P + slot) * W * RP + tu;
                 float coupling = 0.f;
                 for (int w2 = 0; w2 < W; w2++) coupling += rp[w2 * RP];
                 const float2 n = act ? nz[(size_t)sub * R] : make_float2(0.f, 0.f);
