@@ -99,6 +99,7 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
     const int node = r0 + lr;
     const bool act = lr < r_own;
     const bool owner = act && rep == 0;  // writes outputs
+    const bool every_warp_owns = (W - 1) * RPW < r_own;  // the last warp holds a node of this CTA
     const long long kSpin = 1ll << 26;
 
     // every CTA of the cluster is running before any distributed shared memory access
@@ -211,7 +212,12 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
         for (int sub = 0; sub < 10; sub++) {
             if (!skip_wait && !late) late = !wait_s(cur);
             skip_wait = false;
-            __syncthreads();  // all threads are past this phase: arm the buffer's next one
+            // A warp sends its nodes' next S_E only after all its lanes have read
+            // buffer cur and passed its wait, and the other CTAs need every node's
+            // S_E before this buffer's next phase can fill: where every warp of
+            // the CTA owns a node, no block barrier is needed here.  A CTA with
+            // a warp that owns none (the last rank of some shapes) keeps one.
+            if (!every_warp_owns) __syncthreads();
             if (threadIdx.x == 0 && !late)
                 asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(sbar_local + 8u * cur),
                              "r"(4 * N)
