@@ -6,7 +6,8 @@ Every kind of shape the autotuner can pick is forced once (BNM_B200_SHAPE):
 the register-SC kernel (N <= 128) at N = 67, 68 and 100, where each lane's SC
 block is narrower than its 16-byte-aligned S_E stride (18 of 20, 18 of 20 and
 26 of 28 columns; N = 67 with a partly filled last warp), and at N = 128 with
-full 32-column blocks, with one and two particles per CTA; and for 128 < N <= 512 the
+full 32-column blocks, with one and two particles per CTA; the shape the
+autotuner picks at the smallest and largest cluster sizes (N = 130, 512); and for 128 < N <= 512 the
 thread-block-cluster kernels, row-split (1, 2, 4 and 8 CTAs per particle, 8
 or 16 nodes per warp) and column-split (2 to 7 rows per lane, 8 to 25 column pairs per
 warp, one-CTA clusters with a local S_E exchange included, one or two
@@ -33,8 +34,10 @@ SETUPS = {
     "n68": (68, 12000, 500, 2, 6, 2, 3, 3),
     "n100": (100, 15000, 500, 2, 10, 2, 10, 3),
     "n128": (128, 11000, 500, 2, 6, 2, 3, 2),
+    "n130": (130, 11000, 500, 2, 6, 2, 2, 3),
     "n160": (160, 15000, 500, 2, 10, 2, 10, 3),
     "n400": (400, 11000, 500, 2, 6, 2, 2, 2),
+    "n512": (512, 10500, 500, 2, 6, 2, 0, 2),
 }
 # kind,slots,csize,rpw,kr: kind 0 register-SC (slots particles per CTA); kind 1 row-split (rpw nodes per warp, kr chunks in registers); kind 3
 # column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers); kind 4
@@ -53,6 +56,10 @@ SHAPES = {
     "n400": ["1,0,4,8,4", "1,0,8,8,8", "1,0,8,16,4", "3,25,4,4,8", "3,13,8,2,13", "3,25,8,2,25",
              "4,25,4,4,25", "4,25,4,4,20", "4,13,8,2,13"],
 }
+# "auto": the shape the autotuner picks (the smallest and largest node counts of the cluster
+# kernels, N = 130 and 512)
+SHAPES["n130"] = ["auto"]
+SHAPES["n512"] = ["auto"]
 KINDS = {0: "register", 1: "cluster", 3: "colsplit", 4: "colsplit2"}
 
 
@@ -91,13 +98,19 @@ def cases(port):
 @pytest.mark.parametrize("name,shape", [(k, s) for k in SHAPES for s in SHAPES[k]])
 def test_cluster_shape_matches_fp64_oracle(name, shape, cases, monkeypatch):
     c = cases[name]
-    monkeypatch.setenv("BNM_B200_SHAPE", shape)
+    if shape == "auto":
+        monkeypatch.delenv("BNM_B200_SHAPE", raising=False)
+    else:
+        monkeypatch.setenv("BNM_B200_SHAPE", shape)
     with B.Plan(c["cfg"], c["sc"], c["emp_fc"], c["emp_fcd"], host_noise=c["noise"]) as p:
         r = p.run(c["G"], c["wEE"], c["wEI"], c["wie0"] if not c["cfg"].do_fic else None)
         info = p.integrator()
-    k = [int(v) for v in shape.split(",")]
-    assert info["kind"] == KINDS[k[0]], info
-    assert (info["slots"], info["csize"], info["rpw"], info["kr"]) == tuple(k[1:]), info
+    if shape == "auto":
+        assert info["kind"] in ("cluster", "colsplit", "colsplit2") and info["tried"] >= 2, info
+    else:
+        k = [int(v) for v in shape.split(",")]
+        assert info["kind"] == KINDS[k[0]], info
+        assert (info["slots"], info["csize"], info["rpw"], info["kr"]) == tuple(k[1:]), info
     same = (r["fic_ntrials"] == c["trials"]) & (np.abs(r["w_ie"] - c["wIE"]).max(1) < 1e-4)
     assert same.sum() >= 1, (r["fic_ntrials"], c["trials"])
     span = np.ptp(c["bold"], axis=1, keepdims=True) + 1e-12
