@@ -95,6 +95,7 @@ def lib():
         L.bnm_group_last.argtypes = [vp, vp, vp]
         L.bnm_plan_noise.argtypes = [vp, C.c_int64, C.c_int64, vp]
         L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
+        L.bnm_bw_math_probe.argtypes = [i32, vp, i32, vp]
         L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
         L.bnm_run_simulations.argtypes = [vp] * 8 + [i32] * 6 + [vp, i32, vp, i32, i32, i32, i32, vp, i32, i32, i32,
                                                                  vp, vp, vp, vp]
@@ -349,6 +350,15 @@ def measure_fp32_peak(device: int = 0) -> float:
     t = C.c_double()
     _check(lib().bnm_measure_fp32_peak(device, C.byref(t)))
     return t.value
+
+
+def bw_math_probe(x, device: int = 0) -> np.ndarray:
+    """[n, 4]: the Balloon-Windkessel step's e^x - 1 and ln(1 + x) next to
+    CUDA's expm1f and log1pf (test support)."""
+    x = np.ascontiguousarray(x, dtype=np.float32)
+    out = np.zeros((len(x), 4), np.float32)
+    _check(lib().bnm_bw_math_probe(device, _ptr(x), len(x), _ptr(out)))
+    return out
 
 
 def gof_noalloc(d_bold: int, n: int, frames: int, nodes: int, n_vols_remove: int, window_size: int,

@@ -6,6 +6,7 @@
 #include <cuda_runtime.h>
 #include "../../include/bnm_b200.h"
 #include "kernels.h"
+#include "fp32_model.cuh"
 
 int bnm_fail_cuda(cudaError_t e, const char* expr, const char* file, int line);
 
@@ -51,5 +52,35 @@ extern "C" int bnm_measure_fp32_peak(int32_t device, double* tflops) {
     BNM_CUDA_TRY(err);
     const double flops = (double)grid * block * iters * 8 * 2 * 2;
     *tflops = flops / (best * 1e-3) / 1e12;
+    return BNM_OK;
+}
+
+// expm1_bw / log1p_bw (the Balloon-Windkessel step's e^y - 1 and ln(1 + x))
+// next to CUDA's expm1f / log1pf on the same inputs.
+__global__ void bw_math_probe_kernel(const float* x, int n, float* out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float v = x[i];
+    out[4 * i + 0] = bnm::expm1_bw(v);
+    out[4 * i + 1] = expm1f(v);
+    out[4 * i + 2] = bnm::log1p_bw(v);
+    out[4 * i + 3] = log1pf(v);
+}
+
+extern "C" int bnm_bw_math_probe(int32_t device, const float* x, int32_t n, float* out4) {
+    if (!x || !out4 || n < 1) return BNM_EINVAL;
+    BNM_CUDA_TRY(cudaSetDevice(device));
+    float *dx = nullptr, *dout = nullptr;
+    BNM_CUDA_TRY(cudaMalloc(&dx, (size_t)n * sizeof(float)));
+    cudaError_t e = cudaMalloc(&dout, (size_t)n * 4 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(dx, x, (size_t)n * sizeof(float), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        bw_math_probe_kernel<<<(n + 255) / 256, 256>>>(dx, n, dout);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out4, dout, (size_t)n * 4 * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(dx);
+    if (dout) cudaFree(dout);
+    BNM_CUDA_TRY(e);
     return BNM_OK;
 }

@@ -209,6 +209,12 @@ int bnm_plan_integrator(bnm_plan *plan, int32_t *out5, int32_t *n_tried);
  * counterpart in the reference. */
 int bnm_measure_fp32_peak(int32_t device, double *tflops);
 
+/* Test support, no counterpart in the reference: for each of the n inputs x,
+ * out4 receives the FP32 integrators' Balloon-Windkessel e^x - 1 and
+ * ln(1 + x) next to CUDA's expm1f and log1pf ([4 i .. 4 i + 3] = expm1_bw,
+ * expm1f, log1p_bw, log1pf). */
+int bnm_bw_math_probe(int32_t device, const float *x, int32_t n, float *out4);
+
 /* Device noise table of the plan, copied out (n floats from offset). */
 int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);
 
