@@ -302,9 +302,9 @@ def run_b200(args):
             "gpu_launches": launches,
             "roofline": {"bound": "fp32", "kernel": "integrate_fast_kernel", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": 178.9e6 * (T_MS + 1) / 20001,
+                         "traffic": 172.6e6 * (T_MS + 1) / 20001,
                          "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel on "
-                                           "the same workload at 20 s model time (178.9 MB), scaled by model "
+                                           "the same workload at 20 s model time (172.6 MB), scaled by model "
                                            "time (profiles/integrate_fast_kernel_N100_dram_traffic.md)",
                          "peak_source": "measured on this GPU by bnm_measure_fp32_peak (packed FP32 FMA chains)",
                          "work": "2*N^2 FLOP per substep per particle (coupling FMAs only), FIC restarts included"},
