@@ -79,6 +79,17 @@ def test_env_configuration_like_the_reference():
     assert float(vals[4]) == 1.5
 
 
+def test_gram_arithmetic_defaults_to_auto():
+    """The C default (bnm_config_default) and the Python default agree: the
+    Gram arithmetic is chosen by precision when the plan is made (split BF16
+    tensor-core Grams for the FP32 path, FP32 / FP64 SIMT analysis for the
+    reference-order precisions)."""
+    assert B.Config().gram == B.GRAM_AUTO
+    assert B.Config.from_env().gram == B.GRAM_AUTO
+    for g in (B.GRAM_AUTO, B.GRAM_F32, B.GRAM_BF16, B.GRAM_BF16_SPLIT):  # accepted by the size check
+        B.Config(nodes=10, time_steps=60000, bold_tr=1000, window_size=4, gram=g).sizes()
+
+
 def test_no_device_is_an_error_not_a_crash():
     if B.lib().bnm_device_count() > 0:
         pytest.skip("a GPU is present")
