@@ -43,10 +43,10 @@ SETUPS = {
 # column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers); kind 4
 # column-split with two particles per cluster
 SHAPES = {
-    "n67": ["0,1,0,0,0"],
+    "n67": ["0,1,0,0,0", "0,2,0,0,0"],
     "n68": ["0,1,0,0,0", "0,2,0,0,0"],
     "n100": ["0,1,0,0,0", "0,2,0,0,0"],
-    "n128": ["0,1,0,0,0"],
+    "n128": ["0,1,0,0,0", "0,2,0,0,0"],
     "n160": ["1,0,1,8,4", "1,0,2,8,5", "1,0,4,16,4", "1,0,8,8,4",
              "3,10,2,4,10", "3,8,4,2,8", "3,13,2,4,8",
              # one-CTA clusters: S_E exchanged through local shared memory
