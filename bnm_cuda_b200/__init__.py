@@ -96,6 +96,7 @@ def lib():
         L.bnm_plan_noise.argtypes = [vp, C.c_int64, C.c_int64, vp]
         L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
         L.bnm_bw_math_probe.argtypes = [i32, vp, i32, vp]
+        L.bnm_wait_probe.argtypes = [i32, C.c_int64, vp, vp]
         L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
         L.bnm_run_simulations.argtypes = [vp] * 8 + [i32] * 6 + [vp, i32, vp, i32, i32, i32, i32, vp, i32, i32, i32,
                                                                  vp, vp, vp, vp]
@@ -359,6 +360,17 @@ def bw_math_probe(x, device: int = 0) -> np.ndarray:
     out = np.zeros((len(x), 4), np.float32)
     _check(lib().bnm_bw_math_probe(device, _ptr(x), len(x), _ptr(out)))
     return out
+
+
+def wait_probe(limit_ns: int, device: int = 0) -> dict:
+    """bnm_wait_probe: a bounded device wait on an mbarrier that nothing
+    arrives on, with a limit of ``limit_ns`` ns of wall time (test support).
+    Returns the call's status code, the kernel's status word and the elapsed
+    wait in ms; the expected code is BNM_ETIMEOUT."""
+    st, ms = C.c_int32(0), C.c_double(0.0)
+    rc = lib().bnm_wait_probe(device, int(limit_ns), C.byref(st), C.byref(ms))
+    return {"code": rc, "status": st.value, "elapsed_ms": ms.value,
+            "message": lib().bnm_last_error().decode() if rc else ""}
 
 
 def gof_noalloc(d_bold: int, n: int, frames: int, nodes: int, n_vols_remove: int, window_size: int,

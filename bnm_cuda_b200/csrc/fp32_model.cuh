@@ -36,9 +36,23 @@ __device__ __forceinline__ uint32_t smem_addr(const void* p) {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));
 }
 
-// Bounded wait on an mbarrier phase; returns false if it gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long max_iter) {
-    for (long long i = 0; i < max_iter; i++) {
+// Wall-clock limit of every bounded wait in the integrators: a copy or an
+// exchange normally lands within microseconds.
+constexpr long long kWaitNs = 1000000000ll;  // 1 s
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Wait on an mbarrier phase for at most limit_ns nanoseconds of wall time
+// (%globaltimer, read every 16 unsuccessful polls; try_wait itself may suspend
+// the thread for a hardware-defined interval, so the bound is on time, not on
+// polls).  Returns false if it gave up.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long long limit_ns) {
+    unsigned long long t0 = 0;
+    for (uint32_t i = 0;; i++) {
         uint32_t ok;
         asm volatile(
             "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
@@ -46,8 +60,14 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, long lo
             : "r"(bar), "r"(parity)
             : "memory");
         if (ok) return true;
+        if ((i & 15) == 0) {
+            const unsigned long long t = global_ns();
+            if (i == 0)
+                t0 = t;
+            else if ((long long)(t - t0) > limit_ns)
+                return false;
+        }
     }
-    return false;
 }
 
 // e^y - 1 for the Balloon-Windkessel step.  Near zero, where e^y - 1 cancels,

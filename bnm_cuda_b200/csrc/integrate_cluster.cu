@@ -100,7 +100,7 @@ __global__ void integrate_cluster_kernel(SimArgs a, int R) {
     const bool act = lr < r_own;
     const bool owner = act && rep == 0;  // writes outputs
     const bool every_warp_owns = (W - 1) * RPW < r_own;  // the last warp holds a node of this CTA
-    const long long kSpin = 1ll << 26;
+    const long long kSpin = kWaitNs;  // wall-clock limit of each bounded wait
 
     // every CTA of the cluster is running before any distributed shared memory access
     cluster_sync();

@@ -119,7 +119,7 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
     const bool act = tu < r_own;  // thread owns node r0 + tu of its particle
     const bool wr = act && live;  // ... and writes its outputs
     const bool solo = csize == 1;  // S_E exchange through local shared memory
-    const long long kSpin = 1ll << 26;
+    const long long kSpin = kWaitNs;  // wall-clock limit of each bounded wait
 
     cluster_sync();  // every CTA of the cluster runs before any distributed shared memory access
     if (t == 0) {

@@ -85,7 +85,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     const int j = threadIdx.x;  // node owned after the reduce-scatter (32w + lane)
     const bool act = j < N;
     const int pos_j = K * (j / KC) + j % KC;  // S_E buffer slot of node j
-    const long long kSpin = 1ll << 26;
+    const long long kSpin = kWaitNs;  // wall-clock limit of each bounded wait
 
     // ---- barriers; stage SC into shared memory with one TMA bulk copy ----
     if (threadIdx.x == 0) {

@@ -106,6 +106,7 @@ extern "C" int bnm_gof_noalloc(const float* d_bold, int32_t n, int32_t frames, i
     const int corr_len = frames - n_vols_remove;
     if (corr_len < 2) return bnm_fail_msg(BNM_EINVAL, "fewer than 2 frames after removal");
     const int P = N * (N - 1) / 2 - (exc_interhem ? (N / 2) * (N / 2) : 0);
+    if (P < 2) return bnm_fail_msg(BNM_EINVAL, "fewer than 2 node pairs (FC correlation undefined)");
     if (n_emp_fc != P) return bnm_fail_msg(BNM_EINVAL, "empirical FC length does not match the pair count");
     const int h = window_size / 2, L = 2 * h + 1, first = h, last = corr_len - 1 - h;
     const int W = last >= first ? (last - first) / window_step + 1 : 0;

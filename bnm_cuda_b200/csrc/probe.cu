@@ -9,6 +9,7 @@
 #include "fp32_model.cuh"
 
 int bnm_fail_cuda(cudaError_t e, const char* expr, const char* file, int line);
+int bnm_fail_msg(int code, const char* msg);
 
 __global__ void __launch_bounds__(256) ffma2_probe_kernel(float* out, int iters) {
     float2 a[8];
@@ -82,5 +83,51 @@ extern "C" int bnm_bw_math_probe(int32_t device, const float* x, int32_t n, floa
     cudaFree(dx);
     if (dout) cudaFree(dout);
     BNM_CUDA_TRY(e);
+    return BNM_OK;
+}
+
+// Failure detection of the bounded device waits, exercised without a fault:
+// one CTA initialises an mbarrier that nothing ever arrives on (no bulk copy,
+// no MMA and no other thread is involved) and waits on its first phase with
+// the integrators' own mbar_wait and the given wall-clock limit.  The wait
+// must give up, the kernel records the timeout status and the elapsed time,
+// and returns normally, so the context stays usable.
+__global__ void wait_probe_kernel(long long limit_ns, int* status, unsigned long long* elapsed_ns) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bnm::smem_addr(&bar)) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const unsigned long long t0 = bnm::global_ns();
+    const bool ok = bnm::mbar_wait(bnm::smem_addr(&bar), 0, limit_ns);
+    const unsigned long long t1 = bnm::global_ns();
+    if (__syncthreads_or(!ok) && threadIdx.x == 0) {
+        atomicOr(status, bnm::kStatusTimeout);
+        *elapsed_ns = t1 - t0;
+    }
+}
+
+extern "C" int bnm_wait_probe(int32_t device, int64_t limit_ns, int32_t* status_out, double* elapsed_ms) {
+    if (limit_ns < 0 || limit_ns > bnm::kWaitNs) return bnm_fail_msg(BNM_EINVAL, "wait probe: limit out of range");
+    BNM_CUDA_TRY(cudaSetDevice(device));
+    int* d_status = nullptr;
+    unsigned long long* d_ns = nullptr;
+    BNM_CUDA_TRY(cudaMalloc(&d_status, 2 * sizeof(int) + sizeof(unsigned long long)));  // status, pad, elapsed
+    d_ns = reinterpret_cast<unsigned long long*>(d_status + 2);
+    cudaError_t e = cudaMemset(d_status, 0, sizeof(int) * 2 + sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        wait_probe_kernel<<<1, 64>>>((long long)limit_ns, d_status, d_ns);
+        e = cudaGetLastError();
+    }
+    int status = 0;
+    unsigned long long ns = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&status, d_status, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&ns, d_ns, sizeof(ns), cudaMemcpyDeviceToHost);
+    cudaFree(d_status);
+    BNM_CUDA_TRY(e);
+    if (status_out) *status_out = status;
+    if (elapsed_ms) *elapsed_ms = ns * 1e-6;
+    if (status & bnm::kStatusTimeout) return bnm_fail_msg(BNM_ETIMEOUT, "wait probe: the bounded wait gave up");
     return BNM_OK;
 }

@@ -215,6 +215,16 @@ int bnm_measure_fp32_peak(int32_t device, double *tflops);
  * expm1f, log1p_bw, log1pf). */
 int bnm_bw_math_probe(int32_t device, const float *x, int32_t n, float *out4);
 
+/* Test support, no counterpart in the reference: failure detection of the
+ * library's bounded device waits without a GPU fault.  One CTA waits, with the
+ * integrators' own wait routine, on an mbarrier that nothing arrives on (no
+ * copy or MMA in flight) for limit_ns nanoseconds of wall time
+ * (0 <= limit_ns <= 1e9, the integrators' limit).  The wait gives up, the
+ * kernel records the timeout status and returns normally: the call returns
+ * BNM_ETIMEOUT with *status_out = the status word and *elapsed_ms = the
+ * measured wait, and the device stays usable. */
+int bnm_wait_probe(int32_t device, int64_t limit_ns, int32_t *status_out, double *elapsed_ms);
+
 /* Device noise table of the plan, copied out (n floats from offset). */
 int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);
 
@@ -234,9 +244,13 @@ int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);
  *   stream          a cudaStream_t (NULL = the default stream); the call is
  *                   asynchronous on it.
  * Calls whose intermediates exceed the scratch array fail with BNM_EINVAL.
+ * Calls with fewer than 2 node pairs are rejected with BNM_EINVAL as well.
  * All calls share the array: the call zeroes what it accumulates, but calls
  * that overlap on the GPU race.  The first call on a device looks up the
- * array's address; make it before any stream capture. */
+ * array's address.  emp_fc and emp_fcd_sorted are copied to the device
+ * asynchronously on the stream (usually from pageable memory, which the
+ * runtime stages before the call returns); a call is not meant to be
+ * recorded into a CUDA graph. */
 #define BNM_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 int bnm_gof_noalloc(const float *d_bold, int32_t n, int32_t frames, int32_t nodes, int32_t n_vols_remove,
                     int32_t window_size, int32_t window_step, int32_t exc_interhem, int32_t use_fc_diff,
