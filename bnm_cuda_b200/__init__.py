@@ -97,6 +97,7 @@ def lib():
         L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
         L.bnm_bw_math_probe.argtypes = [i32, vp, i32, vp]
         L.bnm_wait_probe.argtypes = [i32, C.c_int64, vp, vp]
+        L.bnm_calculate_params.argtypes = [i32, i32, i32, vp, dbl, dbl, dbl, dbl, vp, vp, vp, vp, vp]
         L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
         L.bnm_run_simulations.argtypes = [vp] * 8 + [i32] * 6 + [vp, i32, vp, i32, i32, i32, i32, vp, i32, i32, i32,
                                                                  vp, vp, vp, vp]
@@ -360,6 +361,24 @@ def bw_math_probe(x, device: int = 0) -> np.ndarray:
     out = np.zeros((len(x), 4), np.float32)
     _check(lib().bnm_bw_math_probe(device, _ptr(x), len(x), _ptr(out)))
     return out
+
+
+LOCAL_PARAMS = ("wee", "wie", "wei")  # bit order of het_mask (run_CMAES.cpp:252)
+
+
+def calculate_params(nodes: int, G: float, wee: float, wie: float, wei: float, het=(), maps=None, scales=None):
+    """bnm_calculate_params: one particle's G and per-node wEE / wEI / wIE.
+    het: names of the regional parameters among LOCAL_PARAMS; maps [n_maps,
+    nodes]; scales [3, n_maps] (map coefficients per local parameter, in
+    LOCAL_PARAMS order)."""
+    mask = sum(1 << LOCAL_PARAMS.index(h) for h in het)
+    maps = _d(np.zeros((0, nodes)) if maps is None else maps).reshape(-1, nodes)
+    scales = _d(np.zeros((3, max(len(maps), 1))) if scales is None else scales)
+    g, ee, ei, ie = np.zeros(1), np.zeros(nodes), np.zeros(nodes), np.zeros(nodes)
+    _check(lib().bnm_calculate_params(nodes, mask, len(maps), _ptr(maps) if len(maps) else None, float(G),
+                                      float(wee), float(wie), float(wei), _ptr(scales), _ptr(g), _ptr(ee), _ptr(ei),
+                                      _ptr(ie)))
+    return g[0], ee, ei, ie
 
 
 def wait_probe(limit_ns: int, device: int = 0) -> dict:

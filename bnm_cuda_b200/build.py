@@ -38,7 +38,7 @@ CU = {
     "integrate_cluster.cu": [],
     "integrate_colsplit.cu": [],
 }
-CPP = ["cmaes.cpp"]
+CPP = ["cmaes.cpp", "params.cpp"]
 HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h", "fp32_model.cuh", "cluster_util.cuh"]
 
 

@@ -65,40 +65,24 @@ struct Driver {
     std::vector<std::vector<double>> maps;
     bool heterogeneous = false, do_fic = false;
 
-    // run_CMAES.cpp:61-143
+    // run_CMAES.cpp:61-143, through the library's bnm_calculate_params
     void calculate_params(std::map<std::string, double>& cp, int ind, double* G, double* wEE, double* wEI,
                           double* wIE) const {
-        G[ind] = cp["G"];
-        std::map<std::string, double> mn, mx;
-        for (auto& h : het_params) {
-            mn[h] = 1000;
-            mx[h] = -1000;
-        }
-        for (int j = 0; j < nodes; j++) {
-            for (auto& h : het_params) {
-                double scaler = 1;
-                for (size_t m = 0; m < maps.size(); m++) scaler += cp[h + "scale_" + std::to_string(m)] * maps[m][j];
-                double v = cp[h] * scaler;
-                mn[h] = std::min(mn[h], v);
-                mx[h] = std::max(mx[h], v);
-                if (h == "wee") wEE[(size_t)ind * nodes + j] = v;
-                else if (h == "wei") wEI[(size_t)ind * nodes + j] = v;
-                else if (h == "wie") wIE[(size_t)ind * nodes + j] = v;
+        static const char* kLocal[3] = {"wee", "wie", "wei"};  // run_CMAES.cpp:252
+        int mask = 0;
+        std::vector<double> scales(3 * std::max<size_t>(maps.size(), 1), 0.0), flat;
+        for (int k = 0; k < 3; k++)
+            if (std::find(het_params.begin(), het_params.end(), kLocal[k]) != het_params.end()) {
+                mask |= 1 << k;
+                for (size_t m = 0; m < maps.size(); m++)
+                    scales[k * maps.size() + m] = cp[std::string(kLocal[k]) + "scale_" + std::to_string(m)];
             }
-            for (auto& h : homo_params) {
-                if (h == "wee") wEE[(size_t)ind * nodes + j] = cp["wee"];
-                else if (h == "wei") wEI[(size_t)ind * nodes + j] = cp["wei"];
-                else if (h == "wie") wIE[(size_t)ind * nodes + j] = cp["wie"];
-            }
-        }
-        for (auto& h : het_params) {
-            if (mn[h] < 0.001) {
-                for (int j = 0; j < nodes; j++) {
-                    double* arr = h == "wee" ? wEE : (h == "wei" ? wEI : wIE);
-                    arr[(size_t)ind * nodes + j] -= mn[h] - 0.001;
-                }
-            }
-        }
+        for (auto& mp : maps) flat.insert(flat.end(), mp.begin(), mp.end());
+        const size_t o = (size_t)ind * nodes;
+        if (bnm_calculate_params(nodes, mask, (int)maps.size(), flat.empty() ? nullptr : flat.data(), cp["G"],
+                                 cp["wee"], cp["wie"], cp["wei"], scales.data(), G + ind, wEE + o, wEI + o,
+                                 wIE + o) != BNM_OK)
+            die("calculate_params");
     }
 };
 

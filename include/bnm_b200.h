@@ -273,6 +273,18 @@ int bnm_run_simulations(double *corr, double *fic_penalties, const double *G_lis
                         int32_t N_SIMS, const float *noise, int32_t rand_seed, int32_t do_fic, int32_t adjust_fic,
                         int32_t *FIC_failed, int32_t *fic_n_trials, double *BOLD_ex, double *ext_means);
 
+/* Parameter expansion of particle values (calculate_params,
+ * run_CMAES.cpp:61-143): G_out = G; for each local parameter k in the
+ * reference's order (wee, wie, wei; run_CMAES.cpp:252) with bit k of het_mask
+ * set, node j gets base_k * (1 + sum_m scales[k][m] * maps[m][j]), and all
+ * nodes of that parameter are shifted up so that the smallest is 0.001 when
+ * any fell below it; parameters without their bit get the base value on
+ * every node.  maps [n_maps][nodes], scales [3][n_maps] (the map coefficients
+ * "<param>scale_<m>"); both may be NULL when het_mask == 0.  Outputs [nodes]. */
+int bnm_calculate_params(int32_t nodes, int32_t het_mask, int32_t n_maps, const double *maps, double G, double wee,
+                         double wie, double wei, const double *scales, double *G_out, double *w_ee, double *w_ei,
+                         double *w_ie);
+
 /* ------------------------------------------------------------- CMA-ES
  * Host optimiser with the semantics of the reference's CMAES_Points
  * (cmaes.cpp:128-557): Hansen's CMA-ES (2006 "Variante 6" or 2016 "16"),

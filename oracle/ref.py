@@ -59,6 +59,9 @@ def ref_lib(fp32: bool = False):
         lib.ref_cmaes_tell.argtypes = [dp, dp]
         lib.ref_cmaes_best.argtypes = [dp]
         lib.ref_cmaes_state.argtypes = [dp, dp, dp]
+        lib.ref_calculate_params.argtypes = [C.c_int, C.c_int, C.c_int, dp, C.c_double, C.c_double, C.c_double,
+                                             C.c_double, dp, dp, dp, dp, dp]
+        lib.ref_run_cmaes_cpu.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
         _libs[key] = lib
     return _libs[key]
 
@@ -143,6 +146,17 @@ def ref_analytical_fic(SC, G, wEE, wEI, fp32=False):
     out = np.zeros(N)
     unstable = ref_lib(fp32).ref_analytical_fic(_d(SC), N, float(G), _d(wEE), _d(wEI), out)
     return out, bool(unstable)
+
+
+def ref_calculate_params(nodes, het_mask, maps, G, wee, wie, wei, scales, fp32=False):
+    """calculate_params of run_CMAES.cpp:61-143 for one particle.
+    -> (G, wEE [N], wEI [N], wIE [N])."""
+    maps = _d(np.zeros((0, nodes)) if maps is None else maps).reshape(-1, nodes)
+    scales = _d(np.zeros((3, max(len(maps), 1))) if scales is None else scales)
+    g, ee, ei, ie = np.zeros(1), np.zeros(nodes), np.zeros(nodes), np.zeros(nodes)
+    ref_lib(fp32).ref_calculate_params(nodes, het_mask, len(maps), maps if len(maps) else np.zeros(1), G, wee, wie,
+                                       wei, scales, g, ee, ei, ie)
+    return g[0], ee, ei, ie
 
 
 # -------------------------------------------------------------------- port
@@ -252,3 +266,45 @@ def run_isolated(fn, *args, env=None, **kwargs):
 
 def _set_env(env):
     os.environ.update({k: str(v) for k, v in env.items()})
+
+
+def port_final_pass(SC, G, wEE, wEI, wIE_final, *, time_steps, bold_tr, n_vols_remove, step, window_size, emp_fc,
+                    emp_fcd, exc=True, seed=410, noise=None, fp32=False):
+    """The final pass of one simulation, recomputed from its final wIE.
+
+    After the last FIC decision (bnm.cpp:230-289) a simulation either restarts
+    from t = 0 with the adjusted wIE or continues; either way the BOLD it
+    reports comes from one uninterrupted pass from t = 0 with the final wIE and
+    the noise stream from its start (the stream restarts with every trial,
+    bnm.cpp:273-274).  So a simulation whose FIC decisions differ from the
+    oracle's (a node's mean current on the threshold can flip under last-ulp
+    differences) is still checked: this reruns the port with numerical FIC off
+    and wIE = the simulation's own final wIE, and returns its BOLD, FC, FCD
+    and goodness of fit (check_fit.cpp:138-217, FP64)."""
+    r = port_integrate(SC, G, wEE, wEI, np.asarray(wIE_final, np.float64), time_steps=time_steps, bold_tr=bold_tr,
+                       n_vols_remove=n_vols_remove, seed=seed, noise=noise, adjust_fic=False, fp32=fp32)
+    kept = r["bold"][n_vols_remove:]
+    fit = port_gof(kept, step, window_size, emp_fc, emp_fcd, exc=exc)
+    return dict(bold=r["bold"], fc=port_fc_tril(kept, exc), fcd=port_fcd_tril(kept, step, window_size, exc),
+                cost=fit["cost"], ext=r["ext"])
+
+
+def every_particle_reference(dev, ref, trials_ref, wie_ref, *, floor, rerun):
+    """Reference values for every particle of a device batch.
+
+    dev: the device's outputs (fic_ntrials, w_ie); ref: dict of per-particle
+    reference arrays (bold, fc, fcd, cost, ...) from the oracle's own FIC path.
+    Particles whose FIC took the oracle's decisions (same trial count, final
+    wIE equal up to FP32 rounding) keep those; every other particle gets
+    rerun(i, final_wIE) (port_final_pass).  At least `floor` of the particles
+    must take the oracle's decisions.  Returns (reference dict, mask of the
+    particles that took the oracle's decisions)."""
+    same = (np.asarray(dev["fic_ntrials"]) == np.asarray(trials_ref)) & \
+        (np.abs(np.asarray(dev["w_ie"]) - np.asarray(wie_ref)).max(1) < 1e-4)
+    assert same.mean() >= floor, ("FIC decisions differ from the oracle's", dev["fic_ntrials"], trials_ref)
+    out = {k: [np.asarray(v[i]) for i in range(len(same))] for k, v in ref.items()}
+    for i in np.flatnonzero(~same):
+        rr = rerun(i, np.asarray(dev["w_ie"][i]))
+        for k in out:
+            out[k][i] = np.asarray(rr[k])
+    return {k: np.array(v) for k, v in out.items()}, same

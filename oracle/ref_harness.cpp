@@ -3,8 +3,8 @@
  * oracle/Makefile; never linked by the product.
  *
  * Compiles the reference's own, unmodified CPU sources in one translation
- * unit, in the order run_CMAES.cpp:47-59 uses (cmaes.cpp, then bnm.cpp which
- * pulls in fic.cpp, constants.h and check_fit.cpp), against the GSL/libks
+ * unit, through run_CMAES.cpp (which includes cmaes.cpp, helpers.cpp and
+ * bnm.cpp, and bnm.cpp fic.cpp, constants.h and check_fit.cpp), against the GSL/libks
  * stand-ins in oracle/compat, and exposes plain C entry points so the tests
  * can call the reference directly:
  *
@@ -15,6 +15,9 @@
  *   ref_analytical_fic    -> analytical_fic    fic.cpp:130-207
  *   ref_cmaes_*           -> CMAES_Points      cmaes.cpp:128-557, driven the
  *                            way main() drives it (run_CMAES.cpp:667-818)
+ *   ref_calculate_params  -> calculate_params  run_CMAES.cpp:61-143
+ *   ref_run_cmaes_cpu     -> main()            run_CMAES.cpp:177-951 (the CPU
+ *                            driver, argv as on its command line)
  *
  * u_real is double by default and float with -DUSE_FLOATS (constants.h:8-22);
  * the entry points take and return double and convert at the boundary.
@@ -26,8 +29,12 @@
 #include <map>
 #include <vector>
 #include <string>
-#include "cmaes.cpp"
-#include "bnm.cpp"
+/* run_CMAES.cpp itself (CPU build: it includes cmaes.cpp, helpers.cpp and
+ * bnm.cpp, run_CMAES.cpp:47-59), with its main() renamed so that this
+ * library can expose calculate_params and the whole CPU driver. */
+#define main ref_run_cmaes_main
+#include "run_CMAES.cpp"
+#undef main
 
 extern "C" {
 
@@ -247,5 +254,43 @@ void ref_cmaes_state(double *mean_out, double *sigma_out, double *C_out) {
     }
     *sigma_out = sigma;
 }
+
+/* calculate_params (run_CMAES.cpp:61-143, CPU signature) for one particle.
+ * het_mask bit k marks local parameter k of {wee, wie, wei} (run_CMAES.cpp:252)
+ * as regional; scales [3][n_maps] are the map coefficients "<param>scale_<m>". */
+void ref_calculate_params(int nodes, int het_mask, int n_maps, const double *maps, double G, double wee, double wie,
+                          double wei, const double *scales, double *G_out, double *w_ee, double *w_ei,
+                          double *w_ie) {
+    static const char *local[3] = {"wee", "wie", "wei"};
+    std::map<std::string, u_real> cp;
+    cp["G"] = (u_real)G;
+    cp["wee"] = (u_real)wee;
+    cp["wie"] = (u_real)wie;
+    cp["wei"] = (u_real)wei;
+    std::vector<std::string> het, homo;
+    for (int k = 0; k < 3; k++) {
+        if (het_mask >> k & 1) {
+            het.push_back(local[k]);
+            for (int m = 0; m < n_maps; m++)
+                cp[std::string(local[k]) + "scale_" + std::to_string(m)] = (u_real)scales[k * n_maps + m];
+        } else {
+            homo.push_back(local[k]);
+        }
+    }
+    std::vector<std::vector<u_real>> mp(n_maps, std::vector<u_real>(nodes));
+    for (int m = 0; m < n_maps; m++)
+        for (int j = 0; j < nodes; j++) mp[m][j] = (u_real)maps[(size_t)m * nodes + j];
+    std::vector<u_real> g(1), ee(nodes), ei(nodes), ie(nodes);
+    calculate_params(g.data(), ee.data(), ei.data(), ie.data(), cp, 0, nodes, het, homo, mp, false);
+    *G_out = (double)g[0];
+    for (int j = 0; j < nodes; j++) {
+        w_ee[j] = (double)ee[j];
+        w_ei[j] = (double)ei[j];
+        w_ie[j] = (double)ie[j];
+    }
+}
+
+/* The reference's CPU driver (run_CMAES.cpp main()). */
+int ref_run_cmaes_cpu(int argc, char **argv) { return ref_run_cmaes_main(argc, argv); }
 
 } /* extern "C" */

@@ -1,6 +1,6 @@
 """Regenerates the golden fixtures in this directory from the reference itself.
 
-    python tests/golden/make_golden.py            # simulation fixtures
+    python tests/golden/make_golden.py [case ...] # simulation fixtures (all, or the named ones)
     python tests/golden/make_golden.py --cmaes    # CMA-ES fixtures
 
 Needs the reference build in oracle/_ref (``make -C oracle``, which compiles
@@ -36,6 +36,10 @@ CASES = {
     "n10_t12s": dict(N=10, T=12000, TR=1000, ws=4, step=1, remove=2, exc=1, n=6, density=0.5, seed=3),
     "n20_t25s_tr500": dict(N=20, T=25000, TR=500, ws=6, step=2, remove=2, exc=1, n=6, density=0.3, seed=4),
     "n16_t15s_allpairs": dict(N=16, T=15000, TR=1000, ws=3, step=1, remove=1, exc=0, n=4, density=0.4, seed=5),
+    # the single-simulation workload at full size: N = 100 (30 % density SC, seed 0), 65 s at TR 1 s
+    # (66 frames, 5 s removed), window 10 step 2 (26 windows, 325 FCD entries); particle 0 is its
+    # G = 1.5, wEE = 0.21, wEI = 0.15
+    "cfg0_n100_t65s": dict(N=100, T=65000, TR=1000, ws=10, step=2, remove=5, exc=1, n=4, density=0.3, seed=0),
 }
 
 
@@ -125,8 +129,10 @@ def _env(c):
 if __name__ == "__main__" and "--cmaes" not in sys.argv:
     from oracle import ref
 
+    only = [a for a in sys.argv[1:] if a in CASES]
     for name, c in CASES.items():
-        print(ref.run_isolated(_case, name, c, env=_env(c)))
+        if not only or name in only:
+            print(ref.run_isolated(_case, name, c, env=_env(c)))
 
 
 def cmaes_objective(X):

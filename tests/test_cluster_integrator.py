@@ -14,9 +14,10 @@ warp, one-CTA clusters with a local S_E exchange included, one or two
 particles per cluster), with SC in registers only or split between registers
 and shared memory.  Two particles per cluster restart together when either
 one's FIC check fails; the other's results must still be those of a run
-alone, which the per-particle comparison with the oracle checks.  Bar: on
-particles whose numerical FIC took the same decisions, BOLD within 1e-3 of its range, FC / FCD within 1e-3, cost within
-1e-2; wIE equal to the oracle's up to FP32 rounding.
+alone, which the per-particle comparison with the oracle checks.  Bar, on every
+particle: BOLD within 1e-3 of its range, FC / FCD within 1e-3, cost within 1e-2.  At least 90 % of the
+particles must take the oracle's numerical-FIC decisions (wIE equal up to FP32 rounding); any other
+particle is compared with the oracle's final pass from its own final wIE.
 """
 import concurrent.futures as cf
 
@@ -95,8 +96,25 @@ def cases(port):
     return out
 
 
+def _reference_for_every_particle(r, c, port):
+    """The oracle's values for the particles whose numerical FIC took its
+    decisions (at least 90 % of them, all in these small batches); the
+    oracle's final pass from the device's own final wIE for the others."""
+    cfg = c["cfg"]
+    s = cfg.sizes()
+    ref = dict(bold=c["bold"], fc=c["fc"], fcd=c["fcd"], cost=c["cost"])
+
+    def rerun(i, wie):
+        return port.port_final_pass(c["sc"], c["G"][i], c["wEE"][i], c["wEI"][i], wie, time_steps=cfg.time_steps,
+                                    bold_tr=cfg.bold_tr, n_vols_remove=s["n_vols_remove"], step=cfg.window_step,
+                                    window_size=cfg.window_size, emp_fc=c["emp_fc"], emp_fcd=c["emp_fcd"],
+                                    exc=bool(cfg.exc_interhem), noise=c["noise"])
+
+    return port.every_particle_reference(r, ref, c["trials"], c["wIE"], floor=0.9, rerun=rerun)
+
+
 @pytest.mark.parametrize("name,shape", [(k, s) for k in SHAPES for s in SHAPES[k]])
-def test_cluster_shape_matches_fp64_oracle(name, shape, cases, monkeypatch):
+def test_cluster_shape_matches_fp64_oracle(name, shape, cases, port, monkeypatch):
     c = cases[name]
     if shape == "auto":
         monkeypatch.delenv("BNM_B200_SHAPE", raising=False)
@@ -111,14 +129,13 @@ def test_cluster_shape_matches_fp64_oracle(name, shape, cases, monkeypatch):
         k = [int(v) for v in shape.split(",")]
         assert info["kind"] == KINDS[k[0]], info
         assert (info["slots"], info["csize"], info["rpw"], info["kr"]) == tuple(k[1:]), info
-    same = (r["fic_ntrials"] == c["trials"]) & (np.abs(r["w_ie"] - c["wIE"]).max(1) < 1e-4)
-    assert same.sum() >= 1, (r["fic_ntrials"], c["trials"])
-    span = np.ptp(c["bold"], axis=1, keepdims=True) + 1e-12
-    err = (np.abs(r["bold"] - c["bold"]) / span).max(axis=(1, 2))
-    assert err[same].max() < 1e-3, err
-    np.testing.assert_allclose(r["fc"][same], c["fc"][same], atol=1e-3)
-    np.testing.assert_allclose(r["fcd"][same], c["fcd"][same], atol=1e-3)
-    np.testing.assert_allclose(r["cost"][same], c["cost"][same], atol=1e-2)
+    ref, same = _reference_for_every_particle(r, c, port)
+    span = np.ptp(ref["bold"], axis=1, keepdims=True) + 1e-12
+    err = (np.abs(r["bold"] - ref["bold"]) / span).max(axis=(1, 2))
+    assert err.max() < 1e-3, (err, same)
+    np.testing.assert_allclose(r["fc"], ref["fc"], atol=1e-3)
+    np.testing.assert_allclose(r["fcd"], ref["fcd"], atol=1e-3)
+    np.testing.assert_allclose(r["cost"], ref["cost"], atol=1e-2)
 
 
 def test_autotuner_picks_a_timed_cluster_shape(cases):

@@ -12,8 +12,11 @@ Tolerances:
     ulp); FIC trial counts and failure flags exact; FC to 1e-6 and FCD
     (window FC and the FCD Gram are FP32 on the device: 1e-4); cost to 1e-4.
   * FP32 product kernel vs the FP64 reference: BOLD to 1e-3 of its range,
-    FC / FCD within 1e-3 absolute (the bar the FP32 product path is held to), cost to 1e-2, on the
-    particles whose numerical FIC took the same decisions (see _same_fic_path).
+    FC / FCD within 1e-3 absolute (the bar the FP32 product path is held to), cost to 1e-2.
+    At least 90 % of the particles must take the reference's numerical-FIC
+    decisions; every other particle is compared with the oracle's final pass
+    from its own final wIE (oracle.ref.port_final_pass), so no particle goes
+    unchecked.
 """
 import numpy as np
 import pytest
@@ -38,7 +41,7 @@ def _plan(g, precision, port, noise_mode=B.NOISE_HOST):
     return B.Plan(cfg, g["sc"], g["emp_fc"], g["emp_fcd"], host_noise=nz)
 
 
-CASES = ["n10_t12s", "n20_t25s_tr500", "n16_t15s_allpairs"]
+CASES = ["n10_t12s", "n20_t25s_tr500", "n16_t15s_allpairs", "cfg0_n100_t65s"]
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -67,14 +70,23 @@ def test_fp64_reference_order_matches_reference(case, golden, port):
     np.testing.assert_allclose(r["ext_means"][:, 2, :], rE_mean, atol=1e-6)
 
 
-def _same_fic_path(r, trials, wie, tol):
-    """Particles whose numerical FIC took the same decisions as the oracle.
-    A node whose mean current sits on the FIC threshold can flip a decision
-    under last-ulp differences (then wIE differs by a whole delta step);
-    those particles are excluded from the trajectory-level comparison."""
-    same = (r["fic_ntrials"] == trials) & (np.abs(r["w_ie"] - wie).max(1) < tol)
-    assert same.mean() >= 0.5, (r["fic_ntrials"], trials)
-    return same
+def _reference_for_every_particle(r, g, port, fp32):
+    """Golden values for the particles whose numerical FIC took the reference's
+    decisions (at least 90 % of them); the oracle's final pass from the
+    device's own final wIE for the others.  A node whose mean current sits on
+    the FIC threshold can flip a decision under last-ulp differences (wIE then
+    differs by a whole delta step)."""
+    N, T, TR, ws, step, remove, exc, nvr, seed = [int(v) for v in g["meta"]]
+    tag = "f32" if fp32 else "f64"
+    ref = dict(bold=g["port_bold"], fc=g["ref_fc"], fcd=g["ref_fcd"], cost=g[f"ref_cost_{tag}"])
+
+    def rerun(i, wie):
+        return port.port_final_pass(g["sc"], g["G"][i], g["wEE"][i], g["wEI"][i], wie, time_steps=T, bold_tr=TR,
+                                    n_vols_remove=nvr, step=step, window_size=ws, emp_fc=g["emp_fc"],
+                                    emp_fcd=g["emp_fcd"], exc=bool(exc), fp32=fp32)
+
+    return port.every_particle_reference(r, ref, g[f"port_trials_{tag}"], g[f"port_wIE_{tag}"], floor=0.9,
+                                         rerun=rerun)
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -83,12 +95,12 @@ def test_fp32_reference_order_matches_float_build(case, golden, port):
     build integrates Balloon-Windkessel states near 1.0 in float, which turns
     last-ulp differences between CUDA's and glibc's expf/powf into 1e-3..1e-1
     relative BOLD differences, so this mode is compared at the cost level
-    (median difference below 1e-2, none above 0.1)."""
+    (median difference below 1e-2, none above 0.1), on every particle."""
     g = golden[case]
     with _plan(g, B.PREC_F32_REF, port) as p:
         r = p.run(g["G"], g["wEE"], g["wEI"])
-    same = _same_fic_path(r, g["port_trials_f32"], g["port_wIE_f32"], 1e-4)
-    d = np.abs(r["cost"] - g["ref_cost_f32"])[same]
+    ref, same = _reference_for_every_particle(r, g, port, fp32=True)
+    d = np.abs(r["cost"] - ref["cost"])
     assert np.median(d) < 1e-2 and d.max() < 0.1, d
     np.testing.assert_allclose(r["fic_penalty"][same], g["ref_pen_f32"][same], atol=3e-2)
 
@@ -97,18 +109,19 @@ def test_fp32_reference_order_matches_float_build(case, golden, port):
 @pytest.mark.parametrize("case", CASES)
 def test_fp32_product_path_within_tolerance_of_fp64(case, slots, golden, port, monkeypatch):
     """slots: particles integrated per CTA by the register kernel (the launcher
-    picks 1 or 2 from the batch size; forced here to cover both)."""
+    picks 1 or 2 from the batch size; forced here to cover both).  Every
+    particle is compared."""
     monkeypatch.setenv("BNM_B200_SLOTS", slots)
     g = golden[case]
     with _plan(g, B.PREC_F32, port) as p:
         r = p.run(g["G"], g["wEE"], g["wEI"])
-    same = _same_fic_path(r, g["port_trials_f64"], g["port_wIE_f64"], 1e-4)
-    span = np.ptp(g["port_bold"], axis=1, keepdims=True) + 1e-12
-    err = (np.abs(r["bold"] - g["port_bold"]) / span).max(axis=(1, 2))
-    assert err[same].max() < 1e-3, err
-    np.testing.assert_allclose(r["fc"][same], g["ref_fc"][same], atol=1e-3)
-    np.testing.assert_allclose(r["fcd"][same], g["ref_fcd"][same], atol=1e-3)
-    np.testing.assert_allclose(r["cost"][same], g["ref_cost_f64"][same], atol=1e-2)
+    ref, same = _reference_for_every_particle(r, g, port, fp32=False)
+    span = np.ptp(ref["bold"], axis=1, keepdims=True) + 1e-12
+    err = (np.abs(r["bold"] - ref["bold"]) / span).max(axis=(1, 2))
+    assert err.max() < 1e-3, (err, same)
+    np.testing.assert_allclose(r["fc"], ref["fc"], atol=1e-3)
+    np.testing.assert_allclose(r["fcd"], ref["fcd"], atol=1e-3)
+    np.testing.assert_allclose(r["cost"], ref["cost"], atol=1e-2)
 
 
 @pytest.mark.parametrize("case", CASES)
@@ -147,9 +160,9 @@ def test_one_shot_run_simulations_mirror(golden, port):
                                 want_bold=True)
     finally:
         del os.environ["BNM_BOLD_REMOVE"]
-    same = out["fic_n_trials"] == g["port_trials_f64"]
-    assert same.mean() >= 0.5
-    np.testing.assert_allclose(out["corr"][same], g["ref_cost_f64"][same], atol=1e-2)
+    ref, same = _reference_for_every_particle({"fic_ntrials": out["fic_n_trials"], "w_ie": out["w_IE_fic"]}, g,
+                                              port, fp32=False)
+    np.testing.assert_allclose(out["corr"], ref["cost"], atol=1e-2)
     np.testing.assert_allclose(out["w_IE_fic"][same], g["port_wIE_f64"][same], atol=1e-4)
 
 

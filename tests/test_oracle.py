@@ -13,7 +13,7 @@ live.
 import numpy as np
 import pytest
 
-CASES = ["n10_t12s", "n20_t25s_tr500", "n16_t15s_allpairs"]
+CASES = ["n10_t12s", "n20_t25s_tr500", "n16_t15s_allpairs", "cfg0_n100_t65s"]
 
 
 def _meta(g):
@@ -43,9 +43,15 @@ def test_port_matches_reference_text_outputs(case, golden, port):
     np.testing.assert_array_equal(g["port_trials_f64"], g["ref_ntrials"])
     np.testing.assert_array_equal(g["port_failed_f64"], g["ref_failed"])
     # the extended r_E series (bnm.cpp:212-226) against a fresh port run
-    for i in range(len(g["G"])):
-        o = port.port_integrate(g["sc"], g["G"][i], g["wEE"][i], g["wEI"][i], g["ref_wIE_analytic"][i],
-                                time_steps=T, bold_tr=TR, n_vols_remove=nvr, seed=seed)
+    import concurrent.futures as cf
+
+    def one(i):
+        return port.port_integrate(g["sc"], g["G"][i], g["wEE"][i], g["wEI"][i], g["ref_wIE_analytic"][i],
+                                   time_steps=T, bold_tr=TR, n_vols_remove=nvr, seed=seed)
+
+    with cf.ThreadPoolExecutor(len(g["G"])) as ex:  # the port releases the GIL
+        outs = list(ex.map(one, range(len(g["G"]))))
+    for i, o in enumerate(outs):
         np.testing.assert_array_equal(o["bold"], g["port_bold"][i])
         np.testing.assert_allclose(o["ext"][2], g["ref_rE_txt"][i][nvr:].mean(0), atol=1e-6)
 
@@ -158,3 +164,50 @@ def test_live_reference_vs_port():
     c, p, c2, p2 = ref.run_isolated(_live_case, env={"BNM_BOLD_REMOVE": 2})
     np.testing.assert_array_equal(c, c2)
     np.testing.assert_array_equal(p, p2)
+
+
+@pytest.mark.parametrize("het", [(), ("wee",), ("wei",), ("wee", "wei"), ("wee", "wie", "wei")])
+def test_calculate_params_matches_reference_bit_for_bit(het):
+    """The library's parameter expansion (bnm_calculate_params, used by the
+    run_CMAES_gpu driver) against the reference's own calculate_params
+    (run_CMAES.cpp:61-143, compiled unmodified in oracle/_ref): base values,
+    per-node map scaling base * (1 + sum_m coef_m map_m[j]) and the shift of
+    a regional parameter whose smallest node value falls below 0.001.  Maps
+    of both kinds the driver accepts (min-max normalised to [0, 1] and
+    z-scored), coefficients drawn across the driver's scale bounds, so both
+    shifted and unshifted expansions occur."""
+    from oracle import ref
+
+    if not ref.ref_available():
+        pytest.skip("reference build missing (make -C oracle)")
+    import bnm_cuda_b200 as B
+
+    rng = np.random.default_rng(11)
+    N = 100
+    shifted = 0
+    for trial in range(40):
+        n_maps = 1 + trial % 3
+        maps = []
+        for m in range(n_maps):
+            x = rng.standard_normal(N)
+            maps.append((x - x.min()) / (x.max() - x.min()) if m % 2 == 0 else (x - x.mean()) / x.std())
+        maps = np.array(maps)
+        # coefficient ranges as run_CMAES.cpp:272-289 derives them (min-max maps: [0, scale_max_minmax];
+        # z-scored: [ceil(-1/max, 0.01), floor(-1/min, 0.01)]), stretched a little past them
+        zs = np.arange(n_maps) % 2 == 1
+        lo, hi = np.full(n_maps, -0.5), np.full(n_maps, 5.0)
+        lo[zs] = np.ceil(-1 / maps[zs].max(1) / 0.01) * 0.01 - 0.2
+        hi[zs] = np.floor(-1 / maps[zs].min(1) / 0.01) * 0.01 + 0.2
+        scales = rng.uniform(lo, hi, (3, n_maps))
+        G, wee, wie, wei = rng.uniform(0.5, 4), rng.uniform(0.001, 0.75), rng.uniform(0, 2), rng.uniform(0.001, 0.75)
+        mask = sum(1 << B.LOCAL_PARAMS.index(h) for h in het)
+        want = ref.ref_calculate_params(N, mask, maps, G, wee, wie, wei, scales)
+        got = B.calculate_params(N, G, wee, wie, wei, het=het, maps=maps, scales=scales)
+        assert got[0] == want[0]
+        for a, b in zip(got[1:], want[1:]):
+            np.testing.assert_array_equal(a, b)
+        for h in het:
+            k = {"wee": 1, "wei": 2, "wie": 3}[h]
+            shifted += int(np.isclose(want[k].min(), 0.001))
+    if het:
+        assert shifted > 0  # the 0.001 shift was exercised
