@@ -62,6 +62,9 @@ def ref_lib(fp32: bool = False):
         lib.ref_calculate_params.argtypes = [C.c_int, C.c_int, C.c_int, dp, C.c_double, C.c_double, C.c_double,
                                              C.c_double, dp, dp, dp, dp, dp]
         lib.ref_run_cmaes_cpu.argtypes = [C.c_int, C.POINTER(C.c_char_p)]
+        lib.ref_run_particles_timed.argtypes = [dp, dp, dp, dp, dp, dp, dp, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                C.c_int, C.c_int, dp, C.c_int, dp, C.c_int, C.c_int, C.c_int,
+                                                C.c_int, C.c_char_p, dp]
         _libs[key] = lib
     return _libs[key]
 
@@ -115,6 +118,26 @@ def ref_run_simulations(SC, G, wEE, wEI, wIE, *, time_steps, bold_tr, rand_seed,
                                       int(no_fcd), window_step, window_size, out_prefix.encode(), 0,
                                       int(save_output), int(extended_output))
     return cost, pen
+
+
+def ref_run_particles_timed(SC, G, wEE, wEI, wIE, *, time_steps, bold_tr, rand_seed, max_fic_trials, emp_fc,
+                            emp_fcd, window_step, window_size, out_dir="", sim_only=False, fp32=False):
+    """The reference's run_simulations loop (bnm.cpp:441-465), one bnm() per
+    particle under OpenMP, timed per particle.  With out_dir, each particle's
+    save_output files go to <out_dir>/p<i>_* and the reference's own FIC trial
+    counts are read back from them.  -> dict(cost, fic_penalty, seconds,
+    trials or None)."""
+    n, N = len(G), SC.shape[0]
+    cost, pen, sec = np.zeros(n), np.zeros(n), np.zeros(n)
+    ref_lib(fp32).ref_run_particles_timed(cost, pen, _d(G), _d(wEE).ravel(), _d(wEI).ravel(), _d(wIE).ravel(),
+                                          _d(SC), N, n, time_steps, bold_tr, rand_seed, max_fic_trials, _d(emp_fc),
+                                          len(emp_fc), _d(emp_fcd), len(emp_fcd), window_step, window_size,
+                                          int(sim_only), out_dir.encode(), sec)
+    trials = None
+    if out_dir:
+        trials = np.array([int(open(os.path.join(out_dir, f"p{i}_fic_ntrials.txt")).read().split()[0])
+                           for i in range(n)])
+    return dict(cost=cost, fic_penalty=pen, seconds=sec, trials=trials)
 
 
 def ref_fc_tril(bold, exc=True, fp32=False):

@@ -290,6 +290,49 @@ void ref_calculate_params(int nodes, int het_mask, int n_maps, const double *map
     }
 }
 
+/* The body of run_simulations' OpenMP loop (bnm.cpp:441-465: one bnm() call
+ * per particle, same arguments), with each particle's wall time recorded and,
+ * when out_dir is given, each particle's save_output files written under its
+ * own prefix <out_dir>/p<i> (run_simulations gives every particle the same
+ * prefix), so that the reference's own FIC trial counts can be read back
+ * (<prefix>_fic_ntrials.txt, bnm.cpp:301-309).  Used to time full-length
+ * simulations of the reference's CPU path. */
+void ref_run_particles_timed(double *corr, double *fic_penalties, const double *G_list, const double *w_EE_list,
+                             const double *w_EI_list, const double *w_IE_list, const double *SC, int nodes,
+                             int N_SIMS, int time_steps, int BOLD_TR, int rand_seed, int max_fic_trials,
+                             const double *emp_fc, int n_emp_fc, const double *emp_fcd, int n_emp_fcd,
+                             int window_step, int window_size, int sim_only, const char *out_dir, double *seconds) {
+    std::vector<u_real> G(N_SIMS), wee((size_t)N_SIMS * nodes), wei((size_t)N_SIMS * nodes),
+        wie((size_t)N_SIMS * nodes), sc((size_t)nodes * nodes), pen(N_SIMS, 0);
+    for (int i = 0; i < N_SIMS; i++) G[i] = (u_real)G_list[i];
+    for (size_t i = 0; i < (size_t)N_SIMS * nodes; i++) {
+        wee[i] = (u_real)w_EE_list[i];
+        wei[i] = (u_real)w_EI_list[i];
+        wie[i] = (u_real)w_IE_list[i];
+    }
+    for (size_t i = 0; i < (size_t)nodes * nodes; i++) sc[i] = (u_real)SC[i];
+    gsl_matrix *sc_gsl = gsl_matrix_alloc(nodes, nodes);
+    for (int i = 0; i < nodes; i++)
+        for (int j = 0; j < nodes; j++) gsl_matrix_set(sc_gsl, i, j, sc[(size_t)i * nodes + j]);
+    gsl_vector *efc = to_gslv(emp_fc, n_emp_fc);
+    gsl_vector *efcd = to_gslv(emp_fcd, n_emp_fcd);
+    const bool save = out_dir && *out_dir;
+#pragma omp parallel for
+    for (int i = 0; i < N_SIMS; i++) {
+        const std::string prefix = save ? std::string(out_dir) + "/p" + std::to_string(i) : std::string("");
+        const double t0 = omp_get_wtime();
+        corr[i] = bnm(nodes, sc.data(), sc_gsl, G[i], wee.data() + (size_t)i * nodes, wei.data() + (size_t)i * nodes,
+                      wie.data() + (size_t)i * nodes, pen.data() + i, true, time_steps, BOLD_TR, rand_seed,
+                      max_fic_trials, efc, efcd, sim_only != 0, false, window_step, window_size, prefix, false, save,
+                      false);
+        seconds[i] = omp_get_wtime() - t0;
+    }
+    for (int i = 0; i < N_SIMS; i++) fic_penalties[i] = (double)pen[i];
+    gsl_vector_free(efc);
+    gsl_vector_free(efcd);
+    gsl_matrix_free(sc_gsl);
+}
+
 /* The reference's CPU driver (run_CMAES.cpp main()). */
 int ref_run_cmaes_cpu(int argc, char **argv) { return ref_run_cmaes_main(argc, argv); }
 
