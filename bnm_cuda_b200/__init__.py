@@ -97,6 +97,8 @@ def lib():
         L.bnm_measure_fp32_peak.argtypes = [i32, C.POINTER(C.c_double)]
         L.bnm_bw_math_probe.argtypes = [i32, vp, i32, vp]
         L.bnm_wait_probe.argtypes = [i32, C.c_int64, vp, vp]
+        L.bnm_plan_graph.argtypes = [vp, vp]
+        L.bnm_philox_probe.argtypes = [i32, vp, i32, vp]
         L.bnm_calculate_params.argtypes = [i32, i32, i32, vp, dbl, dbl, dbl, dbl, vp, vp, vp, vp, vp]
         L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
         L.bnm_run_simulations.argtypes = [vp] * 8 + [i32] * 6 + [vp, i32, vp, i32, i32, i32, i32, vp, i32, i32, i32,
@@ -274,6 +276,12 @@ class Plan:
         _check(lib().bnm_last_gram(self._h, _ptr(t), C.byref(k)))
         return dict(fc_gram_ms=float(t[0]), fcd_gram_ms=float(t[1]), launches=k.value)
 
+    def graph_launched(self) -> bool:
+        """Whether the last run was one CUDA graph launch (bnm_plan_graph)."""
+        g = C.c_int32()
+        _check(lib().bnm_plan_graph(self._h, C.byref(g)))
+        return bool(g.value)
+
     def integrator(self) -> dict:
         """FP32 integrator shape the autotuner picked for the last batch size."""
         o, t = np.zeros(5, np.int32), C.c_int32()
@@ -379,6 +387,15 @@ def calculate_params(nodes: int, G: float, wee: float, wie: float, wei: float, h
                                       float(wee), float(wie), float(wei), _ptr(scales), _ptr(g), _ptr(ee), _ptr(ei),
                                       _ptr(ie)))
     return g[0], ee, ei, ie
+
+
+def philox_probe(counters_keys, device: int = 0) -> np.ndarray:
+    """Device Philox4x32-10 block function: [n, 6] (counter[4], key[2]) ->
+    [n, 4] output words (test support)."""
+    x = np.ascontiguousarray(counters_keys, dtype=np.uint32).reshape(-1, 6)
+    out = np.zeros((len(x), 4), np.uint32)
+    _check(lib().bnm_philox_probe(device, _ptr(x), len(x), _ptr(out)))
+    return out
 
 
 def wait_probe(limit_ns: int, device: int = 0) -> dict:

@@ -170,6 +170,10 @@ struct bnm_plan {
            *io_fcc = nullptr, *io_fcdiff = nullptr, *io_ks = nullptr, *io_wie = nullptr;
     int *io_failed = nullptr, *io_trials = nullptr, *io_unstable = nullptr, *io_status = nullptr;
     bool capturing = false;
+    // bnm_run's generation as one CUDA graph (captured for batches of run_graph_n particles)
+    cudaGraph_t run_graph = nullptr;
+    cudaGraphExec_t run_exec = nullptr;
+    int run_graph_n = 0, last_graph = 0;
     double timings[6] = {0, 0, 0, 0, 0, 0};
     // tensor-core Gram kernels alone: one event pair per launch (FC, then each FCD chunk)
     std::vector<cudaEvent_t> gev;
@@ -190,6 +194,8 @@ extern "C" void bnm_plan_destroy(bnm_plan* p) {
     cudaSetDevice(p->cfg.device);
     if (p->st) cudaStreamSynchronize(p->st);
     for (void* a : p->allocs) cudaFree(a);
+    if (p->run_exec) cudaGraphExecDestroy(p->run_exec);
+    if (p->run_graph) cudaGraphDestroy(p->run_graph);
     if (p->pinned) cudaFreeHost(p->pinned);
     for (auto& e : p->ev)
         if (e) cudaEventDestroy(e);
@@ -822,6 +828,82 @@ static SimArgs sim_args(bnm_plan* p, int n) {
     return a;
 }
 
+static int ensure_pinned(bnm_plan* p);
+static int enqueue_run(bnm_plan* p, int n);
+static int read_timings(bnm_plan* p);
+
+// A generation of a plan whose integrator is already tuned for n particles,
+// with analytic FIC on the device: parameters staged through pinned host
+// buffers, then one graph launch (the same stream operations as the eager
+// path: parameter upload, analytic FIC, integrator, window FC, Grams, KS,
+// goodness of fit, result download), captured on the first such call for n.
+// Optional large outputs (BOLD, FC, FCD, extended means) are copied from the
+// device buffers after the launch.
+static int run_graph(bnm_plan* p, int n, const double* G, const double* w_ee, const double* w_ei,
+                     bnm_batch_out* out) {
+    const bnm_config& c = p->cfg;
+    const bnm_sizes& s = p->sz;
+    const int N = c.nodes;
+    int rc = ensure_pinned(p);
+    if (rc) return rc;
+    for (int i = 0; i < n; i++) {
+        if (!std::isfinite(G[i])) return fail(BNM_EINVAL, "G[%d] is not finite", i);
+        p->io_G[i] = G[i];
+    }
+    for (size_t i = 0; i < (size_t)n * N; i++) {
+        if (!std::isfinite(w_ee[i]) || !std::isfinite(w_ei[i])) return fail(BNM_EINVAL, "wEE/wEI not finite at %zu", i);
+        p->io_wEE[i] = w_ee[i];
+        p->io_wEI[i] = w_ei[i];
+    }
+    cudaStream_t st = p->st;
+    if (!p->run_exec || p->run_graph_n != n) {
+        if (p->run_exec) cudaGraphExecDestroy(p->run_exec);
+        if (p->run_graph) cudaGraphDestroy(p->run_graph);
+        p->run_exec = nullptr;
+        p->run_graph = nullptr;
+        p->run_graph_n = 0;
+        BNM_CUDA_TRY(cudaStreamBeginCapture(st, cudaStreamCaptureModeRelaxed));
+        p->capturing = true;
+        rc = enqueue_run(p, n);
+        p->capturing = false;
+        cudaGraph_t graph = nullptr;
+        const cudaError_t e_end = cudaStreamEndCapture(st, &graph);
+        if (rc) {
+            if (graph) cudaGraphDestroy(graph);
+            return rc;
+        }
+        BNM_CUDA_TRY(e_end);
+        p->run_graph = graph;
+        BNM_CUDA_TRY(cudaGraphInstantiate(&p->run_exec, graph, 0));
+        p->run_graph_n = n;
+    }
+    BNM_CUDA_TRY(cudaGraphLaunch(p->run_exec, st));
+    p->last_graph = 1;
+    if (out->bold) rc = f2d(out->bold, p->d_bold, (size_t)n * s.frames * N, st);
+    if (!rc) rc = d2h(out->ext_means, p->d_ext, (size_t)n * 6 * N, st);
+    if (!rc) rc = f2d(out->fc, p->d_fc, (size_t)n * s.n_pairs, st);
+    if (!rc && !c.no_fcd) rc = f2d(out->fcd, p->d_fcd, (size_t)n * s.n_fcd, st);
+    if (rc) return rc;
+    BNM_CUDA_TRY(cudaStreamSynchronize(st));
+    if ((rc = read_timings(p))) return rc;
+    const int status = *p->io_status;
+    if (status & kStatusTimeout) return fail(BNM_ETIMEOUT, "a device wait gave up (status %d)", status);
+    if (status) return fail(BNM_ECUDA, "device status %d", status);
+    auto put = [](auto* dst, const auto* src, size_t cnt) {
+        if (dst) std::copy(src, src + cnt, dst);
+    };
+    put(out->cost, p->io_cost, n);
+    put(out->fic_penalty, p->io_pen, n);
+    put(out->fc_corr, p->io_fcc, n);
+    put(out->fc_diff, p->io_fcdiff, n);
+    put(out->fcd_ks, p->io_ks, n);
+    put(out->w_ie, p->io_wie, (size_t)n * N);
+    put(out->fic_failed, p->io_failed, n);
+    put(out->fic_ntrials, p->io_trials, n);
+    put(out->fic_unstable, p->io_unstable, n);
+    return BNM_OK;
+}
+
 extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_ee, const double* w_ei,
                        const double* w_ie, bnm_batch_out* out) {
     if (!p || !out || !G || !w_ee || !w_ei) return fail(BNM_EINVAL, "null argument");
@@ -832,12 +914,17 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     if (!c.do_fic && !w_ie) return fail(BNM_EINVAL, "w_ie is required when do_fic == 0");
     BNM_CUDA_TRY(cudaSetDevice(c.device));
     const bool hemis = out->fcd_left || out->fcd_right;
+    const bool device_fic = c.do_fic && !w_ie;
+    // after the first (tuning) run of a batch size, the generation is one graph launch
+    const char* ge = std::getenv("BNM_B200_GRAPH");
+    if (device_fic && !hemis && c.precision == BNM_PREC_F32 && p->tuned_n == n && !(ge && !std::strcmp(ge, "0")))
+        return run_graph(p, n, G, w_ee, w_ei, out);
+    p->last_graph = 0;
     int rc = hemis ? ensure_hemi(p) : BNM_OK;
     if (rc) return rc;
     if ((rc = upload_params(p, n, G, w_ee, w_ei))) return rc;
     cudaStream_t st = p->st;
     BNM_CUDA_TRY(cudaEventRecord(p->ev[0], st));
-    const bool device_fic = c.do_fic && !w_ie;
     p->launches = device_fic ? 2 : 1;  // analytic FIC, integrator
     if (device_fic) {
         if ((rc = launch_fic(p, n))) return rc;
@@ -1216,6 +1303,12 @@ extern "C" int bnm_last_gram(bnm_plan* p, double* ms2, int32_t* launches) {
     ms2[0] = p->gram_ms[0];
     ms2[1] = p->gram_ms[1];
     if (launches) *launches = p->launches;
+    return BNM_OK;
+}
+
+extern "C" int bnm_plan_graph(bnm_plan* p, int32_t* graph_launched) {
+    if (!p || !graph_launched) return fail(BNM_EINVAL, "null argument");
+    *graph_launched = p->last_graph;
     return BNM_OK;
 }
 

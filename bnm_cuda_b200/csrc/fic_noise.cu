@@ -233,3 +233,36 @@ cudaError_t bnm_launch_philox(float* out, uint64_t n, uint64_t seed, int num_sms
     philox_fill_kernel<<<num_sms * 8, 256, 0, st>>>(out, n, seed);
     return cudaGetLastError();
 }
+
+// Known-answer support: the raw Philox4x32-10 block function of the noise
+// source on the device, for n (counter[4], key[2]) inputs.
+namespace bnm {
+__global__ void philox_probe_kernel(const uint32_t* in6, int n, uint32_t* out4) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t c[4] = {in6[6 * i], in6[6 * i + 1], in6[6 * i + 2], in6[6 * i + 3]};
+    philox4x32_10(c, in6[6 * i + 4], in6[6 * i + 5]);
+    for (int k = 0; k < 4; k++) out4[4 * i + k] = c[k];
+}
+}  // namespace bnm
+
+#include "../../include/bnm_b200.h"
+int bnm_fail_cuda(cudaError_t e, const char* expr, const char* file, int line);
+
+extern "C" int bnm_philox_probe(int32_t device, const uint32_t* in6, int32_t n, uint32_t* out4) {
+    if (!in6 || !out4 || n < 1) return BNM_EINVAL;
+    BNM_CUDA_TRY(cudaSetDevice(device));
+    uint32_t *d_in = nullptr, *d_out = nullptr;
+    BNM_CUDA_TRY(cudaMalloc(&d_in, (size_t)n * 6 * 4));
+    cudaError_t e = cudaMalloc(&d_out, (size_t)n * 4 * 4);
+    if (e == cudaSuccess) e = cudaMemcpy(d_in, in6, (size_t)n * 6 * 4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) {
+        bnm::philox_probe_kernel<<<(n + 127) / 128, 128>>>(d_in, n, d_out);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(out4, d_out, (size_t)n * 4 * 4, cudaMemcpyDeviceToHost);
+    cudaFree(d_in);
+    if (d_out) cudaFree(d_out);
+    BNM_CUDA_TRY(e);
+    return BNM_OK;
+}

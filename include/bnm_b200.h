@@ -143,9 +143,18 @@ typedef struct bnm_batch_out {
  * goodness of fit and FIC penalty for n <= max_sims particles.
  * G [n]; w_ee, w_ei [n][nodes].  w_ie [n][nodes]: the fixed wIE when
  * do_fic == 0; with do_fic it is the analytic-FIC starting point (as the
- * reference GPU driver's w_IE_fic), or NULL to compute it on the device. */
+ * reference GPU driver's w_IE_fic), or NULL to compute it on the device.
+ * The reference launches seven kernels with a device synchronisation after
+ * each (bnm.cu:624-724).  Here the first call for a batch size runs eagerly
+ * and tunes the integrator; with the FP32 path and device FIC (w_ie NULL, no
+ * hemisphere FCDs) every later call for that batch size is one CUDA graph
+ * launch of the whole generation (parameter upload from pinned staging,
+ * analytic FIC, integrator, window FC, Grams, KS, fit, result download),
+ * captured on its first use; BNM_B200_GRAPH=0 keeps every call eager. */
 int bnm_run(bnm_plan *plan, int32_t n, const double *G, const double *w_ee, const double *w_ei, const double *w_ie,
             bnm_batch_out *out);
+/* Whether the plan's last bnm_run was a graph launch (1) or eager (0). */
+int bnm_plan_graph(bnm_plan *plan, int32_t *graph_launched);
 
 /* Analytic FIC alone (fic.cpp:130-207) for n particles on the device. */
 int bnm_analytic_fic(bnm_plan *plan, int32_t n, const double *G, const double *w_ee, const double *w_ei,
@@ -224,6 +233,12 @@ int bnm_bw_math_probe(int32_t device, const float *x, int32_t n, float *out4);
  * BNM_ETIMEOUT with *status_out = the status word and *elapsed_ms = the
  * measured wait, and the device stays usable. */
 int bnm_wait_probe(int32_t device, int64_t limit_ns, int32_t *status_out, double *elapsed_ms);
+
+/* Test support, no counterpart in the reference: the Philox4x32-10 block
+ * function (Salmon et al., SC'11) of the noise source, run on the device for
+ * n inputs in6[i] = {counter[0..3], key[0..1]}; out4[i] = the four output
+ * words.  For a known-answer test against the published vectors. */
+int bnm_philox_probe(int32_t device, const uint32_t *in6, int32_t n, uint32_t *out4);
 
 /* Device noise table of the plan, copied out (n floats from offset). */
 int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);

@@ -94,3 +94,36 @@ def test_group_rejects_bad_inputs():
         B.Group([plans[0], plans[0]])
     for p in plans:
         p.close()
+
+
+@pytest.mark.parametrize("N", [48, 160])
+def test_single_plan_generation_is_one_graph_launch(N, monkeypatch):
+    """bnm_run: the first call for a batch size runs eagerly (and tunes the
+    integrator); later calls with device FIC are one graph launch of the whole
+    generation.  The graph must give the eager path's results (same tuned
+    shape, same stream operations), with and without the optional BOLD / FC /
+    FCD outputs, for new parameters as well, and its stage timings must be
+    valid."""
+    sc = synth.make_sc(N, 0.3, 3)
+    cfg = B.Config(nodes=N, max_sims=6, time_steps=12000, bold_tr=500, window_size=10, window_step=2,
+                   bold_remove_s=2)
+    s = cfg.sizes()
+    rng = np.random.default_rng(1)
+    emp_fc, emp_fcd = rng.uniform(-0.2, 0.8, s["n_pairs"]), rng.uniform(-0.3, 1.0, 300)
+    P1, P2 = synth.uniform_params(6, N, 40), synth.uniform_params(6, N, 41)
+    with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+        e1 = p.run(*P1)
+        assert not p.graph_launched()
+        g1 = p.run(*P1, outputs=("w_ie",))
+        assert p.graph_launched()
+        _same(e1, g1)
+        g2 = p.run(*P2)  # full outputs through the graph
+        assert p.graph_launched()
+        t = p.timings()
+        assert t["integrate"] > 0 and t["total"] >= t["integrate"]
+        monkeypatch.setenv("BNM_B200_GRAPH", "0")
+        e2 = p.run(*P2)
+        assert not p.graph_launched()
+    _same(e2, g2)
+    for k in ("bold", "fc", "fcd", "ext_means"):
+        np.testing.assert_array_equal(e2[k], g2[k], err_msg=k)
