@@ -39,7 +39,8 @@ CU = {
     "integrate_colsplit.cu": [],
 }
 CPP = ["cmaes.cpp", "params.cpp"]
-HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h", "fp32_model.cuh", "cluster_util.cuh"]
+HEADERS = ["bnm_common.cuh", "integrate_generic.cuh", "kernels.h", "fp32_model.cuh", "cluster_util.cuh",
+           "noise.cuh"]
 
 
 def _newer(src_paths, out):

@@ -47,7 +47,10 @@ struct SimArgs {
     const double* wEE;     // [n][N]
     const double* wEI;     // [n][N]
     const double* wIE;     // [n][N] initial wIE (analytic FIC or fixed)
-    const float* noise;    // [(T+1)*10][N][2] standard normals
+    const float* noise;    // [(T+1)*10][N][2] standard normals, or NULL: drawn in the kernel (Philox, noise.cuh)
+    uint64_t noise_seed;   // Philox key when noise == NULL
+    int noise_ld;          // node stride of the noise table (N, or N + 1 when padded for an odd N)
+    int n_real;            // nodes of the simulation; the kernel's N may add one padding node
     const float* sc_f32;   // [N][sc_ld] row-major, zero padded
     const double* sc_f64;  // [N][N]
     int sc_ld;

@@ -133,6 +133,7 @@ struct bnm_plan {
     bnm_config cfg;
     bnm_sizes sz;
     int num_sms = 0, kmax = 0, sc_ld = 0, m = 0;
+    int pad = 0, noise_ld = 0;  // padding node of an odd N (column-split kernel); node stride of the noise table
     cudaStream_t st = nullptr;
     cudaEvent_t ev[6] = {}, tev[2] = {};
     double emp_fc_mean = 0;
@@ -242,8 +243,11 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
     // SC: FP32 rows padded for the register kernel, FP64 for the exact kernel,
     // and the FIC copy rounded like the chosen precision's u_real.
     p->kmax = (cfg->precision == BNM_PREC_F32) ? bnm_fast_kmax(N) : 0;
-    p->sc_ld = p->kmax ? p->kmax : N;
-    std::vector<float> sc32((size_t)N * p->sc_ld, 0.f);
+    // an odd N above the register kernel's range runs the column-split kernel
+    // with one padding node (zero SC row and column, its own noise column)
+    p->pad = (cfg->precision == BNM_PREC_F32 && !p->kmax && (N & 1)) ? 1 : 0;
+    p->sc_ld = p->kmax ? p->kmax : N + p->pad;
+    std::vector<float> sc32((size_t)(N + p->pad) * p->sc_ld, 0.f);
     std::vector<double> scfic((size_t)N * N);
     for (int i = 0; i < N; i++)
         for (int j = 0; j < N; j++) {
@@ -258,12 +262,24 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
     BNM_CUDA_TRY(cudaMemcpy(p->d_sc64, sc, (size_t)N * N * 8, cudaMemcpyHostToDevice));
     BNM_CUDA_TRY(cudaMemcpy(p->d_sc_fic, scfic.data(), scfic.size() * 8, cudaMemcpyHostToDevice));
 
-    // noise table
-    BNM_CUDA_TRY(dalloc(p, &p->d_noise, (size_t)s.noise_len));
-    if (cfg->noise_mode == BNM_NOISE_HOST) {
-        BNM_CUDA_TRY(cudaMemcpy(p->d_noise, host_noise, (size_t)s.noise_len * 4, cudaMemcpyHostToDevice));
-    } else {
-        BNM_CUDA_TRY(bnm_launch_philox(p->d_noise, (uint64_t)s.noise_len, cfg->noise_seed, p->num_sms, p->st));
+    // noise: the caller's table, or Philox values drawn where they are consumed
+    // by the register integrator (FP32, N <= 128: no table at all), or a
+    // Philox table for the kernels that read one (BNM_B200_NOISE_TABLE=1
+    // forces the table for the register integrator too)
+    const char* nt = std::getenv("BNM_B200_NOISE_TABLE");
+    const bool table = cfg->noise_mode == BNM_NOISE_HOST || cfg->precision != BNM_PREC_F32 ||
+                       !bnm_fast_kmax(N) || (nt && std::strcmp(nt, "0"));
+    p->noise_ld = N + p->pad;
+    if (table) {
+        const size_t rows = (size_t)(cfg->time_steps + 1) * 10;  // substeps; a row holds (E, I) of every node
+        BNM_CUDA_TRY(dalloc(p, &p->d_noise, rows * p->noise_ld * 2));
+        if (p->pad) BNM_CUDA_TRY(cudaMemset(p->d_noise, 0, rows * p->noise_ld * 2 * 4));
+        if (cfg->noise_mode == BNM_NOISE_HOST)
+            BNM_CUDA_TRY(cudaMemcpy2D(p->d_noise, (size_t)p->noise_ld * 8, host_noise, (size_t)N * 8, (size_t)N * 8,
+                                      rows, cudaMemcpyHostToDevice));
+        else
+            BNM_CUDA_TRY(bnm_launch_philox(p->d_noise, (uint64_t)s.noise_len, N, p->noise_ld, cfg->noise_seed,
+                                           p->num_sms, p->st));
     }
 
     // pair table (run_CMAES.cpp:505-524)
@@ -813,7 +829,10 @@ static SimArgs sim_args(bnm_plan* p, int n) {
     a.wEE = p->d_wEE;
     a.wEI = p->d_wEI;
     a.wIE = p->d_wIE;
-    a.noise = p->d_noise;
+    a.noise = p->d_noise;  // NULL: the register integrator draws Philox noise in place
+    a.noise_seed = c.noise_seed;
+    a.noise_ld = p->noise_ld;
+    a.n_real = c.nodes;
     a.sc_f32 = p->d_sc32;
     a.sc_f64 = p->d_sc64;
     a.sc_ld = p->sc_ld;
@@ -1321,7 +1340,29 @@ extern "C" int bnm_last_timings(bnm_plan* p, double* ms6) {
 extern "C" int bnm_plan_noise(bnm_plan* p, int64_t offset, int64_t n, float* out) {
     if (!p || !out || offset < 0 || n < 0 || offset + n > p->sz.noise_len) return fail(BNM_EINVAL, "bad noise range");
     BNM_CUDA_TRY(cudaSetDevice(p->cfg.device));
-    BNM_CUDA_TRY(cudaMemcpy(out, p->d_noise + offset, (size_t)n * 4, cudaMemcpyDeviceToHost));
+    const int N = p->cfg.nodes;
+    if (p->d_noise && p->noise_ld == N) {
+        BNM_CUDA_TRY(cudaMemcpy(out, p->d_noise + offset, (size_t)n * 4, cudaMemcpyDeviceToHost));
+        return BNM_OK;
+    }
+    // a padded table, or noise drawn in place by the integrator: materialise
+    // the values in the unpadded order
+    std::vector<float> all;
+    const float* src = p->d_noise;
+    float* tmp = nullptr;
+    if (!src) {
+        BNM_CUDA_TRY(cudaMalloc(&tmp, (size_t)p->sz.noise_len * 4));
+        cudaError_t e = bnm_launch_philox(tmp, (uint64_t)p->sz.noise_len, N, N, p->cfg.noise_seed, p->num_sms, 0);
+        if (e == cudaSuccess) e = cudaMemcpy(out, tmp + offset, (size_t)n * 4, cudaMemcpyDeviceToHost);
+        cudaFree(tmp);
+        BNM_CUDA_TRY(e);
+        return BNM_OK;
+    }
+    const size_t rows = (size_t)(p->cfg.time_steps + 1) * 10;
+    all.resize((size_t)p->sz.noise_len);
+    BNM_CUDA_TRY(cudaMemcpy2D(all.data(), (size_t)N * 8, src, (size_t)p->noise_ld * 8, (size_t)N * 8, rows,
+                              cudaMemcpyDeviceToHost));
+    std::copy(all.begin() + offset, all.begin() + offset + n, out);
     return BNM_OK;
 }
 

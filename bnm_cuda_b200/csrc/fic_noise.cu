@@ -17,13 +17,14 @@
 // Noise table: the reference draws standard normals in (ms, substep, node,
 // E|I) order, one stream shared by every particle and every FIC trial
 // (run_CMAES.cpp:640-657, bnm.cpp:187-188, 273-274).  The Philox mode keeps
-// those semantics with a counter-based generator: element e of the table is
-// a function of (seed, e) only.  Philox4x32-10 (Salmon et al., SC'11,
-// "Parallel random numbers: as easy as 1, 2, 3") maps counter e/4 to four
-// 32-bit words, turned into four normals by the Box-Muller transform.
+// those semantics with a counter-based generator (noise.cuh): the value for
+// (ms, substep, node, E|I) is a function of the seed and those indices only,
+// so the register integrator draws it in place; the table below holds the
+// same values for the kernels that read one.
 #include <cstdint>
 #include <cuda_runtime.h>
 #include "kernels.h"
+#include "noise.cuh"
 
 namespace bnm {
 
@@ -169,50 +170,22 @@ __global__ void analytic_fic_kernel(FicArgs a) {
 }
 
 // ------------------------------------------------------------- Philox
-__device__ __forceinline__ void philox_round(uint32_t (&c)[4], uint32_t k0, uint32_t k1) {
-    const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
-    const uint32_t hi0 = __umulhi(M0, c[0]), lo0 = M0 * c[0];
-    const uint32_t hi1 = __umulhi(M1, c[2]), lo1 = M1 * c[2];
-    const uint32_t n0 = hi1 ^ c[1] ^ k0, n1 = lo1, n2 = hi0 ^ c[3] ^ k1, n3 = lo0;
-    c[0] = n0; c[1] = n1; c[2] = n2; c[3] = n3;
-}
-
-__device__ __forceinline__ void philox4x32_10(uint32_t (&c)[4], uint32_t k0, uint32_t k1) {
-#pragma unroll
-    for (int r = 0; r < 10; r++) {
-        philox_round(c, k0, k1);
-        k0 += 0x9E3779B9u;
-        k1 += 0xBB67AE85u;
-    }
-}
-
-// Four standard normals for counter `ctr` (table elements 4*ctr .. 4*ctr+3).
-__device__ __forceinline__ float4 philox_normals(uint64_t seed, uint64_t ctr) {
-    uint32_t c[4] = {(uint32_t)ctr, (uint32_t)(ctr >> 32), 0u, 0u};
-    philox4x32_10(c, (uint32_t)seed, (uint32_t)(seed >> 32));
-    const float s = 2.3283064365386963e-10f;  // 2^-32
-    // uniforms in (0, 1]
-    const float u0 = ((float)c[0] + 1.0f) * s, u1 = ((float)c[1] + 0.5f) * s;
-    const float u2 = ((float)c[2] + 1.0f) * s, u3 = ((float)c[3] + 0.5f) * s;
-    const float r0 = sqrtf(-2.0f * logf(fminf(u0, 1.0f))), r1 = sqrtf(-2.0f * logf(fminf(u2, 1.0f)));
-    float s0, c0, s1, c1;
-    sincospif(2.0f * u1, &s0, &c0);
-    sincospif(2.0f * u3, &s1, &c1);
-    return make_float4(r0 * c0, r0 * s0, r1 * c1, r1 * s1);
-}
-
-__global__ void philox_fill_kernel(float* out, uint64_t n, uint64_t seed) {
-    const uint64_t n4 = (n + 3) / 4;
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n4; i += (uint64_t)gridDim.x * blockDim.x) {
-        const float4 v = philox_normals(seed, i);
-        const uint64_t e = 4 * i;
-        if (e + 3 < n) {
-            reinterpret_cast<float4*>(out)[i] = v;
-        } else {
-            if (e < n) out[e] = v.x;
-            if (e + 1 < n) out[e + 1] = v.y;
-            if (e + 2 < n) out[e + 2] = v.z;
-        }
+// The noise table in the reference's array order ([ms][substep][node][E, I],
+// run_CMAES.cpp:640-657): thread i draws Philox counter i = (ms * 5 + pair) *
+// N + node (philox_noise_pair) and writes that node's E and I values of the
+// substeps 2 pair and 2 pair + 1.
+// The table's node stride ld may exceed N (a padding node's column, left as
+// it is); the values depend on N, not on ld.
+__global__ void philox_fill_kernel(float* out, uint64_t n_counters, int N, int ld, uint32_t key0, uint32_t key1) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n_counters;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t q = i / (uint64_t)N;  // ms * 5 + pair
+        const int node = (int)(i - q * (uint64_t)N);
+        const int ms = (int)(q / 5), pair = (int)(q % 5);
+        const float4 v = philox_noise_pair(key0, key1, ms, pair, node, N);
+        const uint64_t e0 = (((uint64_t)ms * 10 + 2 * pair) * ld + node) * 2, e1 = e0 + 2 * (uint64_t)ld;
+        reinterpret_cast<float2*>(out)[e0 / 2] = make_float2(v.x, v.y);
+        reinterpret_cast<float2*>(out)[e1 / 2] = make_float2(v.z, v.w);
     }
 }
 
@@ -229,8 +202,11 @@ cudaError_t bnm_launch_analytic_fic(const FicArgs& a, cudaStream_t st) {
     return cudaGetLastError();
 }
 
-cudaError_t bnm_launch_philox(float* out, uint64_t n, uint64_t seed, int num_sms, cudaStream_t st) {
-    philox_fill_kernel<<<num_sms * 8, 256, 0, st>>>(out, n, seed);
+// n = (T + 1) * 10 * N * 2 values, i.e. (T + 1) * 5 * N Philox counters, into
+// a table of node stride ld >= N.
+cudaError_t bnm_launch_philox(float* out, uint64_t n, int N, int ld, uint64_t seed, int num_sms, cudaStream_t st) {
+    if (N < 1 || ld < N || n % (20 * (uint64_t)N)) return cudaErrorInvalidValue;
+    philox_fill_kernel<<<num_sms * 8, 256, 0, st>>>(out, n / 4, N, ld, (uint32_t)seed, (uint32_t)(seed >> 32));
     return cudaGetLastError();
 }
 

@@ -17,11 +17,12 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return y;
 }
 
-// r = x / (1 - exp(-d x)); for |d x| < 0.1 the quotient is evaluated as
-// (1/d) / P(u) with P(u) = (1 - e^-u)/u truncated after u^4 (rel. err < 2e-8).
-__device__ __forceinline__ float rate(float x, float d, float inv_d, float neg_d_log2e) {
+// r = x / (1 - exp(-d x)) from x and e = exp(-d x) (the caller forms e, so
+// that the exponent's argument need not wait for x); for |d x| < 0.1 the
+// quotient is evaluated as (1/d) / P(u) with P(u) = (1 - e^-u)/u truncated
+// after u^4 (rel. err < 2e-8).
+__device__ __forceinline__ float rate_from(float x, float e, float d, float inv_d) {
     const float u = d * x;
-    const float e = ex2_approx(x * neg_d_log2e);
     float p = fmaf(u, 1.0f / 120.0f, -1.0f / 24.0f);
     p = fmaf(p, u, 1.0f / 6.0f);
     p = fmaf(p, u, -0.5f);
@@ -30,6 +31,10 @@ __device__ __forceinline__ float rate(float x, float d, float inv_d, float neg_d
     const float num = small ? inv_d : x;
     const float den = small ? p : (1.0f - e);
     return num * rcp_approx(den);
+}
+
+__device__ __forceinline__ float rate(float x, float d, float inv_d, float neg_d_log2e) {
+    return rate_from(x, ex2_approx(x * neg_d_log2e), d, inv_d);
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void* p) {

@@ -1,5 +1,9 @@
-// FP32 integrator for 128 < N <= 512, column-split layout: one
-// thread-block cluster per particle, one thread per node for the update.
+// FP32 integrator for 128 < N <= 1024, column-split layout: one
+// thread-block cluster per particle, one thread per node for the update.  An
+// odd node count runs as N + 1 nodes: the padding node has a zero SC row and
+// column (it neither drives nor feels the network), zero weights, its own
+// column of the noise table, no part in the FIC decision and no outputs; the
+// real nodes' results are those of the unpadded system.
 //
 // Same model, time loop, FIC restarts, BOLD and extended outputs as the
 // reference's bnm kernel (bnm.cu:72-315) and CPU path (bnm.cpp:167-290), and
@@ -40,8 +44,9 @@ constexpr int kRing = 4;  // noise ring stages (milliseconds)
 // millisecond: a CTA that saw a wait run out stops issuing copies and waiting
 // but keeps computing and sending until the next agreement point, so every
 // CTA reaches the same points.  A CTA that stopped arming its S_E barriers
-// collects at most kAgreeMs * 5 * 4 N <= 163840 bytes of negative tx-count
-// per barrier (N <= 512), inside the mbarrier's 2^20 - 1 range.
+// collects at most kAgreeMs * 5 * 4 N P bytes of negative tx-count per
+// barrier (P particles per cluster; N <= 1024, P = 2: 655360), inside the
+// mbarrier's 2^20 - 1 range.
 constexpr int kAgreeMs = 16;
 
 // Shared-memory layout (bytes), in this order:
@@ -116,8 +121,10 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
     uint64_t* mbar = reinterpret_cast<uint64_t*>(smem_raw + L::mbar_off(W, R));
 
     const int node = r0 + tu;
+    const int NR = a.n_real;      // nodes of the simulation: an odd count runs with one padding node
     const bool act = tu < r_own;  // thread owns node r0 + tu of its particle
-    const bool wr = act && live;  // ... and writes its outputs
+    const bool real = act && node < NR;  // ... a node of the simulation (not the padding node)
+    const bool wr = real && live;  // ... and writes its outputs
     const bool solo = csize == 1;  // S_E exchange through local shared memory
     const long long kSpin = kWaitNs;  // wall-clock limit of each bounded wait
 
@@ -169,9 +176,10 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
     const float kDtGammaI = C::dt * C::gamma_I, kDtInvTauI = C::dt / C::tau_I;
 
     const float GJ = (float)a.G[sim] * C::J_NMDA;
-    const float wEE = act ? (float)a.wEE[(size_t)sim * N + node] : 0.f;
-    const float wEI = act ? (float)a.wEI[(size_t)sim * N + node] : 0.f;
-    float wIE = act ? (float)a.wIE[(size_t)sim * N + node] : 0.f;
+    // the padding node (zero SC row and column) integrates with zero weights and takes no part in FIC
+    const float wEE = real ? (float)a.wEE[(size_t)sim * NR + node] : 0.f;
+    const float wEI = real ? (float)a.wEI[(size_t)sim * NR + node] : 0.f;
+    float wIE = real ? (float)a.wIE[(size_t)sim * NR + node] : 0.f;
     float delta = (float)a.init_delta;
     float S_E = 0.001f, S_I = 0.001f, IE = 0.f, II = 0.f, rE = 0.f, rI = 0.f;
     double mean_IE = 0.0;
@@ -339,7 +347,7 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
         if (--to_frame == 0) {  // ts % TR == 0
             to_frame = a.TR;
             if (act) {
-                if (live) a.bold[((size_t)sim * a.frames + frame) * N + node] = bw.bold();
+                if (wr) a.bold[((size_t)sim * a.frames + frame) * NR + node] = bw.bold();
                 if (frame >= a.n_vols_remove) {
                     double* e = ext + tu;
                     e[0 * RP] += S_E;
@@ -359,7 +367,7 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
                 const bool my_adj = P == 1 ? adj[0] : (slot ? adj[P - 1] : adj[0]);
                 const int my_trial = P == 1 ? trial[0] : (slot ? trial[P - 1] : trial[0]);
                 bool needs = false;
-                if (act && my_adj) {
+                if (real && my_adj) {
                     const double diff = mean_IE / duration - (double)C::b_a_ratio_E;
                     if (fabs(diff + 0.026) > 0.005) {
                         needs = true;
@@ -431,9 +439,9 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
         }
     }
     if (!timed_out && wr) {
-        a.wIE_out[(size_t)sim * N + node] = (double)wIE;
+        a.wIE_out[(size_t)sim * NR + node] = (double)wIE;
         const double kept = (double)(frame - a.n_vols_remove);
-        for (int e = 0; e < 6; e++) a.ext[((size_t)sim * 6 + e) * N + node] = ext[e * RP + tu] / kept;
+        for (int e = 0; e < 6; e++) a.ext[((size_t)sim * 6 + e) * NR + node] = ext[e * RP + tu] / kept;
     }
     if (!timed_out && crank == 0 && tu == 0 && live) {
         a.trials[sim] = P == 1 ? trial[0] : (slot ? trial[P - 1] : trial[0]);
@@ -482,6 +490,9 @@ const std::vector<Variant>& variants() {
     static const std::vector<Variant> v = {
         BNM_V(8), BNM_V(10), BNM_V(13), BNM_V(16), BNM_V(25), make_variant<5, 10, 10>(), make_variant<6, 12, 12>(),
         make_variant<7, 13, 13>(),
+        // N above 512 (76 to 96 rows per CTA of an 8-CTA cluster): 3 or 4 rows per
+        // lane, 25 column pairs per warp, 12 or 16 of them in registers
+        make_variant<3, 25, 16>(), make_variant<3, 25, 12>(), make_variant<4, 25, 12>(),
         // two particles per cluster
         make_variant<2, 10, 10, 2>(), make_variant<4, 10, 10, 2>(), make_variant<2, 13, 13, 2>(),
         make_variant<4, 13, 13, 2>(), make_variant<2, 16, 16, 2>(), make_variant<4, 16, 16, 2>(),
@@ -510,7 +521,7 @@ using namespace bnm;
 // can run.
 extern "C" int bnm_colsplit_shape(int N, int csize, int rpl, int k2, int krp, int np, int* threads, int* rows,
                                   size_t* smem) {
-    if (N <= 0 || N > 512 || (N & 1) || csize < 1 || csize > 8) return 0;
+    if (N <= 0 || N > 1024 || (N & 1) || csize < 1 || csize > 8) return 0;
     const Variant* v = find(rpl, k2, krp, np);
     if (!v) return 0;
     int R = (N + csize - 1) / csize;

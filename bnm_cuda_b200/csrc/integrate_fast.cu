@@ -35,6 +35,10 @@
 #include <cstdlib>
 #include "kernels.h"
 #include "fp32_model.cuh"
+#include "noise.cuh"
+#ifndef BNM_FAST_CHAIN
+#define BNM_FAST_CHAIN 1  // the folded substep chain below (0: the plain form, kept for comparison)
+#endif
 #define BNM_GENERIC_NS fastgen
 #include "integrate_generic.cuh"
 
@@ -49,7 +53,7 @@ constexpr int kStages = 4;
 
 // Per-particle ("slot") state that every thread keeps for its node.
 struct Slot {
-    float GJ, wEE, wEI, wIE, delta, S_E, S_I, IE, II, rE, rI;
+    float GJ, GJa, GJe, wEE, wEI, wIE, delta, S_E, S_I, IE, II, rE, rI;
     double mean_IE;
     BW bw;
 };
@@ -61,7 +65,12 @@ struct Slot {
 // simulated millisecond per iteration in lockstep but keep their own time,
 // FIC trial and noise stream; a slot whose particle ends takes the next one
 // from the batch's work counter.
-template <int K, int KC, int P>
+//
+// NZI: the noise is drawn in the kernel (Philox, noise.cuh: one call per node
+// and substep pair gives the E and I values of both substeps) instead of
+// being streamed from the table through the TMA ring; the values are the
+// table's, so both give the same results.
+template <int K, int KC, int P, bool NZI>
 __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     static_assert(K % 4 == 0 && K <= 32, "K");
     static_assert(KC % 2 == 0 && KC <= K && KC + 2 >= K, "KC");
@@ -74,7 +83,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     const int N = a.N;
     const uint32_t ms_bytes = (uint32_t)(10 * N * sizeof(float2));
     float2* ring = reinterpret_cast<float2*>(smem_raw);
-    float* sc_stage = reinterpret_cast<float*>(smem_raw + (size_t)P * kStages * ms_bytes);
+    float* sc_stage = reinterpret_cast<float*>(smem_raw + (NZI ? 0 : (size_t)P * kStages * ms_bytes));
     float* S_buf = sc_stage + (size_t)N * LD;
     double* ext = reinterpret_cast<double*>(S_buf + P * 2 * LD);
     uint64_t* mbar = reinterpret_cast<uint64_t*>(ext + (size_t)P * 6 * blockDim.x);
@@ -124,6 +133,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     }
 
     const char* noise_bytes = reinterpret_cast<const char*>(a.noise);
+    const uint32_t key0 = (uint32_t)a.noise_seed, key1 = (uint32_t)(a.noise_seed >> 32);
     const double duration = (double)(a.samp_end - a.samp_start + 1);
     const float SQ = C::sigma_model * C::sqrt_dt;
     const float LOG2E = 1.4426950408889634f;
@@ -164,6 +174,8 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
         const int sm = live[p] ? sim[p] : 0;
         Slot& q = sl[p];
         q.GJ = (float)a.G[sm] * C::J_NMDA;
+        q.GJa = q.GJ * C::a_E;                 // coupling -> a_E I_E - b_E
+        q.GJe = q.GJa * (-C::d_E * LOG2E);     // coupling -> exponent argument of the E rate
         q.wEE = act ? (float)a.wEE[(size_t)sm * N + j] : 0.f;
         q.wEI = act ? (float)a.wEI[(size_t)sm * N + j] : 0.f;
         q.wIE = act ? (float)a.wIE[(size_t)sm * N + j] : 0.f;
@@ -199,25 +211,108 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
 #pragma unroll
         for (int p = 0; p < P; p++) any |= live[p];
         if (!any) break;
-        if (threadIdx.x == 0) {
+        const float2* nz[P];
+        if (!NZI) {
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int p = 0; p < P; p++)
+                    if (live[p]) issue(p);
+            }
+            bool late = false;
 #pragma unroll
             for (int p = 0; p < P; p++)
-                if (live[p]) issue(p);
-        }
-        bool late = false;
+                if (live[p]) late |= !wait_copy(p, c_cons[p]);
+            if (__syncthreads_or(late)) {
+                timed_out = true;
+                break;
+            }
 #pragma unroll
-        for (int p = 0; p < P; p++)
-            if (live[p]) late |= !wait_copy(p, c_cons[p]);
-        if (__syncthreads_or(late)) {
-            timed_out = true;
-            break;
+            for (int p = 0; p < P; p++) nz[p] = ring + ((size_t)p * kStages + c_cons[p] % kStages) * 10 * N + j;
         }
-        const float2* nz[P];
-#pragma unroll
-        for (int p = 0; p < P; p++) nz[p] = ring + ((size_t)p * kStages + c_cons[p] % kStages) * 10 * N + j;
+        float4 npair[P];  // NZI: this node's noise for the current substep pair
 
 #pragma unroll
         for (int sub = 0; sub < 10; sub++) {
+#if BNM_FAST_CHAIN
+            // Rows 1-3 of each lane's slots first: their sums go to the other
+            // lanes of the row group by three independent shuffles, whose
+            // latency then overlaps the FMAs of slot 0 (this lane's own row,
+            // two accumulator chains).
+            float2 acc[P][4], acc0b[P];
+            float4 sv[P][K / 4];
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                acc0b[p] = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int r = 0; r < 4; r++) acc[p][r] = make_float2(0.f, 0.f);
+#pragma unroll
+                for (int c4 = 0; c4 < K / 4; c4++)
+                    sv[p][c4] = reinterpret_cast<const float4*>(S_buf + (p * 2 + cur) * LD + v * K)[c4];
+            }
+#pragma unroll
+            for (int c4 = 0; c4 < K / 4; c4++) {  // pairs 2 c4, 2 c4 + 1 (those below KC / 2)
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    const float2 s01 = make_float2(sv[p][c4].x, sv[p][c4].y), s23 = make_float2(sv[p][c4].z, sv[p][c4].w);
+#pragma unroll
+                    for (int r = 1; r < 4; r++) {
+                        acc[p][r] = __ffma2_rn(sc[r][2 * c4], s01, acc[p][r]);
+                        if (2 * c4 + 1 < KC / 2) acc[p][r] = __ffma2_rn(sc[r][2 * c4 + 1 < KC / 2 ? 2 * c4 + 1 : 0], s23, acc[p][r]);
+                    }
+                }
+            }
+            float rsum[P];
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                // reduce-scatter over the 4 lanes of this row group: lane v ^ m keeps
+                // row v in its slot m, so the three exchanges are independent
+                const float r1 = __shfl_xor_sync(0xffffffffu, acc[p][1].x + acc[p][1].y, 1);
+                const float r2 = __shfl_xor_sync(0xffffffffu, acc[p][2].x + acc[p][2].y, 2);
+                const float r3 = __shfl_xor_sync(0xffffffffu, acc[p][3].x + acc[p][3].y, 3);
+                rsum[p] = r1 + (r2 + r3);
+            }
+#pragma unroll
+            for (int c4 = 0; c4 < K / 4; c4++) {
+#pragma unroll
+                for (int p = 0; p < P; p++) {
+                    const float2 s01 = make_float2(sv[p][c4].x, sv[p][c4].y), s23 = make_float2(sv[p][c4].z, sv[p][c4].w);
+                    float2& a0 = (c4 & 1) ? acc0b[p] : acc[p][0];
+                    a0 = __ffma2_rn(sc[0][2 * c4], s01, a0);
+                    if (2 * c4 + 1 < KC / 2) a0 = __ffma2_rn(sc[0][2 * c4 + 1 < KC / 2 ? 2 * c4 + 1 : 0], s23, a0);
+                }
+            }
+#pragma unroll
+            for (int p = 0; p < P; p++) {
+                Slot& q = sl[p];
+                const float coupling = ((acc[p][0].x + acc0b[p].x) + (acc[p][0].y + acc0b[p].y)) + rsum[p];
+                float2 n;
+                if (NZI) {
+                    if (sub % 2 == 0) npair[p] = philox_noise_pair(key0, key1, ts[p], sub / 2, j, N);
+                    n = sub % 2 == 0 ? make_float2(npair[p].x, npair[p].y) : make_float2(npair[p].z, npair[p].w);
+                } else {
+                    n = act ? nz[p][(size_t)sub * N] : make_float2(0.f, 0.f);
+                }
+                // The dependent chain from the coupling to the new S_E is one FMA to the
+                // exponent's argument, the rate, and one FMA to S_E: every term that does
+                // not involve the coupling is formed beforehand from the old state.
+                const float BE = fmaf(q.wEE, q.S_E, C::w_E__I_0) - q.wIE * q.S_I;  // I_E without coupling
+                const float xB = fmaf(C::a_E, BE, -C::b_E);
+                q.IE = fmaf(q.GJ, coupling, BE);
+                const float xE = fmaf(q.GJa, coupling, xB);  // a_E I_E - b_E
+                const float eE = ex2_approx(fmaf(q.GJe, coupling, xB * (-C::d_E * LOG2E)));
+                q.rE = rate_from(xE, eE, C::d_E, 1.0f / C::d_E);
+                q.II = fmaf(q.wEI, q.S_E, C::w_I__I_0) - q.S_I;
+                q.rI = rate(fmaf(C::a_I, q.II, -C::b_I), C::d_I, 1.0f / C::d_I, -C::d_I * LOG2E);
+                // S += sigma sqrt(dt) xi + dt ((1-S_E) gamma_E r_E - S_E/tau_E), constants folded;
+                // __saturatef clips to [0, 1] and maps NaN to 0 like std::max(0, std::min(S, 1))
+                const float aE = fmaf(-kDtGammaE, q.S_E, kDtGammaE);
+                const float baseE = q.S_E + fmaf(-kDtInvTauE, q.S_E, SQ * n.x);
+                const float dSI = fmaf(kDtGammaI, q.rI, fmaf(-kDtInvTauI, q.S_I, SQ * n.y));
+                q.S_E = __saturatef(fmaf(aE, q.rE, baseE));
+                q.S_I = __saturatef(q.S_I + dSI);
+                if (act) S_buf[(p * 2 + (cur ^ 1)) * LD + pos_j] = q.S_E;
+            }
+#else
             float2 acc[P][4];
 #pragma unroll
             for (int p = 0; p < P; p++)
@@ -246,7 +341,13 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
                 const float r2 = __shfl_xor_sync(0xffffffffu, acc[p][2].x + acc[p][2].y, 2);
                 const float r3 = __shfl_xor_sync(0xffffffffu, acc[p][3].x + acc[p][3].y, 3);
                 const float coupling = ((acc[p][0].x + acc[p][0].y) + r1) + (r2 + r3);
-                const float2 n = act ? nz[p][(size_t)sub * N] : make_float2(0.f, 0.f);
+                float2 n;
+                if (NZI) {
+                    if (sub % 2 == 0) npair[p] = philox_noise_pair(key0, key1, ts[p], sub / 2, j, N);
+                    n = sub % 2 == 0 ? make_float2(npair[p].x, npair[p].y) : make_float2(npair[p].z, npair[p].w);
+                } else {
+                    n = act ? nz[p][(size_t)sub * N] : make_float2(0.f, 0.f);
+                }
                 q.IE = fmaf(q.GJ, coupling, fmaf(q.wEE, q.S_E, C::w_E__I_0)) - q.wIE * q.S_I;
                 q.II = fmaf(q.wEI, q.S_E, C::w_I__I_0) - q.S_I;
                 q.rE = rate(fmaf(C::a_E, q.IE, -C::b_E), C::d_E, 1.0f / C::d_E, -C::d_E * LOG2E);
@@ -260,6 +361,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
                 q.S_I = __saturatef(q.S_I + dSI);
                 if (act) S_buf[(p * 2 + (cur ^ 1)) * LD + pos_j] = q.S_E;
             }
+#endif
             __syncthreads();
             cur ^= 1;
         }
@@ -317,15 +419,17 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
                             frame[p] = 0;
                             to_frame[p] = 1;
                             trial[p]++;
-                            // the copies already in flight hold milliseconds after
-                            // the restart point: let them land, then refetch from 0
-                            if (threadIdx.x == 0) s_flag = (int)c_issue[p];
-                            __syncthreads();
-                            const uint32_t in_flight_end = (uint32_t)s_flag;
-                            bool lt = false;
-                            for (; c_cons[p] < in_flight_end; c_cons[p]++) lt |= !wait_copy(p, c_cons[p]);
-                            if (threadIdx.x == 0) ms_next[p] = 0;
-                            if (__syncthreads_or(lt)) timed_out = true;
+                            if (!NZI) {
+                                // the copies already in flight hold milliseconds after
+                                // the restart point: let them land, then refetch from 0
+                                if (threadIdx.x == 0) s_flag = (int)c_issue[p];
+                                __syncthreads();
+                                const uint32_t in_flight_end = (uint32_t)s_flag;
+                                bool lt = false;
+                                for (; c_cons[p] < in_flight_end; c_cons[p]++) lt |= !wait_copy(p, c_cons[p]);
+                                if (threadIdx.x == 0) ms_next[p] = 0;
+                                if (__syncthreads_or(lt)) timed_out = true;
+                            }
                         } else {
                             failed[p] = true;
                             adjusting[p] = false;
@@ -365,29 +469,40 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     }
 }
 
-template <int K, int KC, int P>
-static cudaError_t launch_fast(const SimArgs& a, int grid, cudaStream_t st) {
-    const int threads = ((a.N + 31) / 32) * 32;
-    const size_t smem = (size_t)P * kStages * 10 * a.N * sizeof(float2) + (size_t)a.N * 4 * K * sizeof(float) +
-                        (size_t)P * 2 * 4 * K * sizeof(float) + (size_t)P * 6 * threads * sizeof(double) +
-                        (1 + P * kStages) * sizeof(uint64_t);
-    cudaError_t e =
-        cudaFuncSetAttribute(integrate_fast_kernel<K, KC, P>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    integrate_fast_kernel<K, KC, P><<<grid, threads, smem, st>>>(a);
-    return cudaGetLastError();
+template <int K, int KC, int P, bool NZI>
+static size_t fast_smem(int N, int threads) {
+    return (NZI ? 0 : (size_t)P * kStages * 10 * N * sizeof(float2)) + (size_t)N * 4 * K * sizeof(float) +
+           (size_t)P * 2 * 4 * K * sizeof(float) + (size_t)P * 6 * threads * sizeof(double) +
+           (1 + P * kStages) * sizeof(uint64_t);
 }
 
 template <int K, int KC, int P>
-static double share_fast(const SimArgs& a, int grid, int num_sms) {
+static cudaError_t launch_fast(const SimArgs& a, int grid, cudaStream_t st) {
     const int threads = ((a.N + 31) / 32) * 32;
-    const size_t smem = (size_t)P * kStages * 10 * a.N * sizeof(float2) + (size_t)a.N * 4 * K * sizeof(float) +
-                        (size_t)P * 2 * 4 * K * sizeof(float) + (size_t)P * 6 * threads * sizeof(double) +
-                        (1 + P * kStages) * sizeof(uint64_t);
+    if (!a.noise) {  // noise drawn in the kernel
+        const size_t smem = fast_smem<K, KC, P, true>(a.N, threads);
+        cudaError_t e = cudaFuncSetAttribute(integrate_fast_kernel<K, KC, P, true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        integrate_fast_kernel<K, KC, P, true><<<grid, threads, smem, st>>>(a);
+        return cudaGetLastError();
+    }
+    const size_t smem = fast_smem<K, KC, P, false>(a.N, threads);
+    cudaError_t e = cudaFuncSetAttribute(integrate_fast_kernel<K, KC, P, false>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    integrate_fast_kernel<K, KC, P, false><<<grid, threads, smem, st>>>(a);
+    return cudaGetLastError();
+}
+
+template <int K, int KC, int P, bool NZI>
+static double share_fast_t(const SimArgs& a, int grid, int num_sms) {
+    const int threads = ((a.N + 31) / 32) * 32;
+    const size_t smem = fast_smem<K, KC, P, NZI>(a.N, threads);
     int per_sm = 0;
-    if (cudaFuncSetAttribute(integrate_fast_kernel<K, KC, P>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    if (cudaFuncSetAttribute(integrate_fast_kernel<K, KC, P, NZI>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, integrate_fast_kernel<K, KC, P>, threads, smem) !=
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, integrate_fast_kernel<K, KC, P, NZI>, threads, smem) !=
             cudaSuccess ||
         per_sm < 1) {
         cudaGetLastError();
@@ -395,6 +510,11 @@ static double share_fast(const SimArgs& a, int grid, int num_sms) {
     }
     const double cap = (double)per_sm * num_sms;
     return grid >= cap ? 1.0 : grid / cap;
+}
+
+template <int K, int KC, int P>
+static double share_fast(const SimArgs& a, int grid, int num_sms) {
+    return a.noise ? share_fast_t<K, KC, P, false>(a, grid, num_sms) : share_fast_t<K, KC, P, true>(a, grid, num_sms);
 }
 
 }  // namespace bnm
@@ -417,6 +537,7 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
     if (sh.kind == 0) {
         const int ld = bnm_fast_kmax(a.N);
         if (!ld || a.sc_ld != ld || (sh.slots != 1 && sh.slots != 2)) return cudaErrorInvalidValue;
+        if (a.noise && a.noise_ld != a.N) return cudaErrorInvalidValue;
         // CTAs are persistent over the batch: two per SM with one slot, one with two
         const int P = sh.slots;
         int grid = (a.n_sims + P - 1) / P;
@@ -434,9 +555,19 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
             default: return cudaErrorInvalidValue;
         }
     }
-    if (sh.kind == 1) return bnm_launch_integrate_cluster(a, sh.csize, sh.rpw, sh.kr, st);
-    if (sh.kind == 3 || sh.kind == 4)
-        return bnm_launch_integrate_colsplit(a, sh.csize, sh.rpw, sh.slots, sh.kr, sh.kind == 4 ? 2 : 1, st);
+    if (!a.noise) return cudaErrorInvalidValue;  // only the register kernel draws its noise in place
+    if (sh.kind == 1) {
+        if (a.noise_ld != a.N) return cudaErrorInvalidValue;
+        return bnm_launch_integrate_cluster(a, sh.csize, sh.rpw, sh.kr, st);
+    }
+    if (sh.kind == 3 || sh.kind == 4) {
+        // an odd node count runs with one padding node: the plan's noise table
+        // and SC carry its column (and SC row)
+        SimArgs b = a;
+        b.N = a.N + (a.N & 1);
+        if (a.noise_ld != b.N || a.sc_ld < b.N) return cudaErrorInvalidValue;
+        return bnm_launch_integrate_colsplit(b, sh.csize, sh.rpw, sh.slots, sh.kr, sh.kind == 4 ? 2 : 1, st);
+    }
     if (sh.kind != 2) return cudaErrorInvalidValue;
     const int threads = ((a.N + 31) / 32) * 32;
     if (threads > 1024) return cudaErrorInvalidValue;
@@ -475,7 +606,7 @@ double bnm_integrator_share(const bnm::SimArgs& a, const bnm::IntegratorShape& s
     }
     if (sh.kind == 1) return bnm_cluster_share(a.N, sh.csize, sh.rpw, sh.kr, a.n_sims);
     if (sh.kind == 3 || sh.kind == 4)
-        return bnm_colsplit_share(a.N, sh.csize, sh.rpw, sh.slots, sh.kr, sh.kind == 4 ? 2 : 1, a.n_sims);
+        return bnm_colsplit_share(a.N + (a.N & 1), sh.csize, sh.rpw, sh.slots, sh.kr, sh.kind == 4 ? 2 : 1, a.n_sims);
     return 1.0;  // the reference-order kernel fills the GPU (two CTAs per SM, persistent)
 }
 
@@ -504,6 +635,7 @@ int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max) {
         }
     int vs[4 * 64];
     const int nv = bnm_colsplit_variants(vs, 64);
+    const int Nc = N + (N & 1);  // column-split shapes of an odd N include one padding node
     for (int cs : {1, 2, 4, 8})
         for (int v = 0; v < nv && v < 64; v++) {
             int threads, rows;
@@ -512,7 +644,7 @@ int bnm_integrator_candidates(int N, bnm::IntegratorShape* out, int max) {
             bool dup = false;  // the variant table repeats (rpl, k2, k2) when k2 <= 8
             for (int u = 0; u < v; u++)
                 dup |= vs[4 * u] == rpl && vs[4 * u + 1] == k2 && vs[4 * u + 2] == krp && vs[4 * u + 3] == np;
-            if (!dup && bnm_colsplit_shape(N, cs, rpl, k2, krp, np, &threads, &rows, &smem))
+            if (!dup && bnm_colsplit_shape(Nc, cs, rpl, k2, krp, np, &threads, &rows, &smem))
                 add({np == 2 ? 4 : 3, k2, cs, rpl, krp});
         }
     add({2, 0, 0, 0, 0});

@@ -67,7 +67,7 @@ __global__ void integrate_generic_kernel(SimArgs a, int sc_in_smem) {
     const bool act = j < N;
     const R* sc_row = SC + (size_t)(act ? j : 0) * ld;
     const unsigned int duration = a.samp_end - a.samp_start + 1;
-    const size_t plane = (size_t)N;
+    const size_t plane = (size_t)a.noise_ld;  // node stride of the noise table
 
     for (;;) {
         __syncthreads();

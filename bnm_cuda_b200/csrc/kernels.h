@@ -187,5 +187,5 @@ cudaError_t bnm_launch_fcd_operand(const bnm::OperandArgs& a, cudaStream_t st);
 cudaError_t bnm_launch_fc_operand(const bnm::OperandArgs& a, cudaStream_t st);
 cudaError_t bnm_launch_gram_tc(const bnm::GramArgs& a, int split, cudaStream_t st);
 cudaError_t bnm_launch_analytic_fic(const bnm::FicArgs& a, cudaStream_t st);
-cudaError_t bnm_launch_philox(float* out, uint64_t n, uint64_t seed, int num_sms, cudaStream_t st);
+cudaError_t bnm_launch_philox(float* out, uint64_t n, int N, int ld, uint64_t seed, int num_sms, cudaStream_t st);
 extern "C" int bnm_fast_kmax(int N);

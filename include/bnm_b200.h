@@ -38,10 +38,13 @@ extern "C" {
  * reference's default double build, F32_REF its USE_FLOATS build. */
 enum { BNM_PREC_F32 = 0, BNM_PREC_F64 = 1, BNM_PREC_F32_REF = 2 };
 
-/* Noise source.  PHILOX: counter-based table keyed by noise_seed, shared by
- * all particles and FIC trials (the reference's common-random-numbers
- * semantics).  HOST: the caller's precomputed table (the reference's
- * mt19937 + normal_distribution<float> stream, run_CMAES.cpp:640-657). */
+/* Noise source.  PHILOX: counter-based Philox4x32-10 + Box-Muller keyed by
+ * noise_seed, shared by all particles and FIC trials (the reference's
+ * common-random-numbers semantics); the FP32 register integrator (N <= 128)
+ * draws the values where it uses them (no table), the other kernels read a
+ * table of the same values.  HOST: the caller's precomputed table (the
+ * reference's mt19937 + normal_distribution<float> stream,
+ * run_CMAES.cpp:640-657). */
 enum { BNM_NOISE_PHILOX = 0, BNM_NOISE_HOST = 1 };
 
 /* Arithmetic of the FC and FCD Grams (both over rows centred and scaled in
@@ -240,7 +243,9 @@ int bnm_wait_probe(int32_t device, int64_t limit_ns, int32_t *status_out, double
  * words.  For a known-answer test against the published vectors. */
 int bnm_philox_probe(int32_t device, const uint32_t *in6, int32_t n, uint32_t *out4);
 
-/* Device noise table of the plan, copied out (n floats from offset). */
+/* The plan's noise in the table's order ([ms][substep][node][E, I]), n floats
+ * from offset: the table when the plan holds one, else the Philox values the
+ * register integrator draws in place (materialised for the copy). */
 int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);
 
 /* ------------------------------------------------ allocation-free entry

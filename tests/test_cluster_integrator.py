@@ -7,7 +7,8 @@ the register-SC kernel (N <= 128) at N = 67, 68 and 100, where each lane's SC
 block is narrower than its 16-byte-aligned S_E stride (18 of 20, 18 of 20 and
 26 of 28 columns; N = 67 with a partly filled last warp), and at N = 128 with
 full 32-column blocks, with one and two particles per CTA; the shape the
-autotuner picks at the smallest and largest cluster sizes (N = 130, 512); and for 128 < N <= 512 the
+autotuner picks at the smallest and largest cluster sizes (N = 130, 512), at odd N (133, 379: the
+column-split kernel with one padding node) and above 512 (600); and for 128 < N <= 512 the
 thread-block-cluster kernels, row-split (1, 2, 4 and 8 CTAs per particle, 8
 or 16 nodes per warp) and column-split (2 to 7 rows per lane, 8 to 25 column pairs per
 warp, one-CTA clusters with a local S_E exchange included, one or two
@@ -39,6 +40,10 @@ SETUPS = {
     "n160": (160, 15000, 500, 2, 10, 2, 10, 3),
     "n400": (400, 11000, 500, 2, 6, 2, 2, 2),
     "n512": (512, 10500, 500, 2, 6, 2, 0, 2),
+    # odd node counts (one padding node in the column-split kernel) and N > 512
+    "n133": (133, 11000, 500, 2, 6, 2, 3, 3),
+    "n379": (379, 11000, 500, 2, 6, 2, 2, 2),
+    "n600": (600, 10500, 500, 2, 6, 2, 0, 2),
 }
 # kind,slots,csize,rpw,kr: kind 0 register-SC (slots particles per CTA); kind 1 row-split (rpw nodes per warp, kr chunks in registers); kind 3
 # column-split (slots column pairs per warp, rpw rows per lane, kr pairs in registers); kind 4
@@ -61,6 +66,9 @@ SHAPES = {
 # kernels, N = 130 and 512)
 SHAPES["n130"] = ["auto"]
 SHAPES["n512"] = ["auto"]
+SHAPES["n133"] = ["auto", "3,10,1,5,10", "4,10,2,4,10"]
+SHAPES["n379"] = ["auto", "4,25,4,4,20"]
+SHAPES["n600"] = ["auto"]
 KINDS = {0: "register", 1: "cluster", 3: "colsplit", 4: "colsplit2"}
 
 

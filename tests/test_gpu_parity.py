@@ -133,6 +133,26 @@ def test_device_analytic_fic_matches_reference(case, golden, port):
     np.testing.assert_allclose(w, g["ref_wIE_analytic"], rtol=1e-10)
 
 
+def test_inline_philox_noise_equals_table(golden, port, monkeypatch):
+    """The register integrator draws its Philox noise in place (no table); the
+    same plan with the table forced (BNM_B200_NOISE_TABLE=1) streams the same
+    values from HBM.  Both must give bit-identical results, and the values the
+    plan reports must be those of the table."""
+    g = golden["n20_t25s_tr500"]
+    a = _plan(g, B.PREC_F32, port, noise_mode=B.NOISE_PHILOX)
+    monkeypatch.setenv("BNM_B200_NOISE_TABLE", "1")
+    b = _plan(g, B.PREC_F32, port, noise_mode=B.NOISE_PHILOX)
+    monkeypatch.delenv("BNM_B200_NOISE_TABLE")
+    n = a.sizes["noise_len"]
+    np.testing.assert_array_equal(a.noise(0, n), b.noise(0, n))
+    ra, rb = a.run(g["G"], g["wEE"], g["wEI"]), b.run(g["G"], g["wEE"], g["wEI"])
+    for k in ("cost", "fic_penalty", "bold", "w_ie", "fcd"):
+        np.testing.assert_array_equal(ra[k], rb[k], err_msg=k)
+    np.testing.assert_array_equal(ra["fic_ntrials"], rb["fic_ntrials"])
+    a.close()
+    b.close()
+
+
 def test_philox_noise_table(golden, port):
     g = golden["n10_t12s"]
     a = _plan(g, B.PREC_F32, port, noise_mode=B.NOISE_PHILOX)
