@@ -497,6 +497,10 @@ extern "C" int bnm_mlp_set_params(bnm_mlp* p, const float* flat) {
     if (!p || !flat) return bnm_fail_msg(BNM_EINVAL, "null argument");
     BNM_CUDA_TRY(cudaSetDevice(p->device));
     BNM_CUDA_TRY(cudaMemcpy(p->w, flat, (size_t)p->n_params * 4, cudaMemcpyHostToDevice));
+    // new parameters start a new optimisation: Adam's moments and step count restart
+    BNM_CUDA_TRY(cudaMemsetAsync(p->m, 0, (size_t)p->n_params * 4, p->st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->v, 0, (size_t)p->n_params * 4, p->st));
+    p->adam_t = 0;
     to_bf16_kernel<<<256, 256, 0, p->st>>>(p->w, p->w16, p->n_params);
     BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
     return BNM_OK;

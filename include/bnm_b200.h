@@ -355,6 +355,7 @@ int bnm_mlp_create(int32_t in_dim, int32_t hidden, int32_t layers, int32_t out_d
 void bnm_mlp_destroy(bnm_mlp *mlp);
 int64_t bnm_mlp_num_params(const bnm_mlp *mlp);
 int bnm_mlp_get_params(bnm_mlp *mlp, float *flat);
+/* Sets every parameter; the optimiser state (Adam moments, step count) restarts. */
 int bnm_mlp_set_params(bnm_mlp *mlp, const float *flat);
 /* epochs of shuffled mini-batches (full batches only); loss_per_epoch may be NULL */
 int bnm_mlp_train(bnm_mlp *mlp, const float *X, const float *Y, int32_t n, int32_t epochs, int32_t batch, float lr,
