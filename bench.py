@@ -665,7 +665,13 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
     ap.add_argument("--particles", type=int, default=N_SIMS, help="profiling knob: particles per GPU")
     ap.add_argument("--model-ms", type=int, default=T_MS, help="profiling knob: model time per simulation")
+    ap.add_argument("--profile", action="store_true",
+                    help="profiling knob: no integrator autotuning (BNM_B200_TUNE=0: the default shape, no timing "
+                         "launches), so that a run's launch order is fixed: the target simulation's kernels, then "
+                         "each step's")
     args = ap.parse_args()
+    if args.profile:
+        os.environ["BNM_B200_TUNE"] = "0"
     if args.particles != N_SIMS or args.model_ms != T_MS:
         N_SIMS, T_MS = args.particles, args.model_ms
         WORKLOAD = f"profiling-case-N100-{T_MS // 1000}s-x{N_SIMS}"

@@ -263,12 +263,18 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
     BNM_CUDA_TRY(cudaMemcpy(p->d_sc_fic, scfic.data(), scfic.size() * 8, cudaMemcpyHostToDevice));
 
     // noise: the caller's table, or Philox values drawn where they are consumed
-    // by the register integrator (FP32, N <= 128: no table at all), or a
-    // Philox table for the kernels that read one (BNM_B200_NOISE_TABLE=1
-    // forces the table for the register integrator too)
+    // by the FP32 integrators (register kernel and both cluster kernels: no
+    // table at all), or a Philox table for the reference-order kernel, which
+    // reads one (also the FP32 path's only kernel where no cluster shape fits
+    // N; BNM_B200_NOISE_TABLE=1 forces the table for every kernel)
     const char* nt = std::getenv("BNM_B200_NOISE_TABLE");
-    const bool table = cfg->noise_mode == BNM_NOISE_HOST || cfg->precision != BNM_PREC_F32 ||
-                       !bnm_fast_kmax(N) || (nt && std::strcmp(nt, "0"));
+    bool fp32_inline = cfg->precision == BNM_PREC_F32 && bnm_fast_kmax(N);
+    if (cfg->precision == BNM_PREC_F32 && !fp32_inline) {
+        IntegratorShape cand[128];
+        const int nc = bnm_integrator_candidates(N, cand, 128);
+        for (int i = 0; i < nc; i++) fp32_inline |= cand[i].kind != 2;
+    }
+    const bool table = cfg->noise_mode == BNM_NOISE_HOST || !fp32_inline || (nt && std::strcmp(nt, "0"));
     p->noise_ld = N + p->pad;
     if (table) {
         const size_t rows = (size_t)(cfg->time_steps + 1) * 10;  // substeps; a row holds (E, I) of every node

@@ -33,6 +33,7 @@
 #include <vector>
 #include "kernels.h"
 #include "fp32_model.cuh"
+#include "noise.cuh"
 #include "cluster_util.cuh"
 
 namespace bnm {
@@ -167,7 +168,8 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
 
     const uint32_t s_local = smem_addr(S_buf);
     const uint32_t flags_local = smem_addr(flags);
-    const char* noise_bytes = reinterpret_cast<const char*>(a.noise);
+    const char* noise_bytes = reinterpret_cast<const char*>(a.noise);  // NULL: Philox noise drawn in place
+    const uint32_t key0 = (uint32_t)a.noise_seed, key1 = (uint32_t)(a.noise_seed >> 32);
     const uint32_t run_bytes = (uint32_t)(r_own * sizeof(float2));  // one substep of the own nodes
     const double duration = (double)(a.samp_end - a.samp_start + 1);
     const float SQ = C::sigma_model * C::sqrt_dt;
@@ -250,8 +252,13 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
     bool late = false;  // sticky; block-uniform after each __syncthreads_or
     int since_agree = 0, n_agree = 0;
     while (ts <= a.T) {
-        if (t == 0 && !late) issue();
-        late = __syncthreads_or(late || !wait_copy(c_cons));
+        if (a.noise) {
+            if (t == 0 && !late) issue();
+            late = __syncthreads_or(late || !wait_copy(c_cons));
+        } else {  // Philox noise drawn by the block instead of copied from a table
+            philox_fill_stage(ring + (size_t)(c_cons % kRing) * 10 * R, R, r0, r_own, a.n_real, ts, key0, key1);
+            late = __syncthreads_or(late);
+        }
         const float2* nz = ring + (size_t)(c_cons % kRing) * 10 * R + (act ? tu : 0);
 
 #pragma unroll 1

@@ -555,9 +555,8 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
             default: return cudaErrorInvalidValue;
         }
     }
-    if (!a.noise) return cudaErrorInvalidValue;  // only the register kernel draws its noise in place
     if (sh.kind == 1) {
-        if (a.noise_ld != a.N) return cudaErrorInvalidValue;
+        if (a.noise && a.noise_ld != a.N) return cudaErrorInvalidValue;
         return bnm_launch_integrate_cluster(a, sh.csize, sh.rpw, sh.kr, st);
     }
     if (sh.kind == 3 || sh.kind == 4) {
@@ -565,10 +564,10 @@ cudaError_t bnm_launch_integrate_shape(const bnm::SimArgs& a, const bnm::Integra
         // and SC carry its column (and SC row)
         SimArgs b = a;
         b.N = a.N + (a.N & 1);
-        if (a.noise_ld != b.N || a.sc_ld < b.N) return cudaErrorInvalidValue;
+        if ((a.noise && a.noise_ld != b.N) || a.sc_ld < b.N) return cudaErrorInvalidValue;
         return bnm_launch_integrate_colsplit(b, sh.csize, sh.rpw, sh.slots, sh.kr, sh.kind == 4 ? 2 : 1, st);
     }
-    if (sh.kind != 2) return cudaErrorInvalidValue;
+    if (sh.kind != 2 || !a.noise) return cudaErrorInvalidValue;  // the reference-order kernel reads a table
     const int threads = ((a.N + 31) / 32) * 32;
     if (threads > 1024) return cudaErrorInvalidValue;
     size_t smem = 2 * (size_t)threads * sizeof(float);

@@ -63,4 +63,19 @@ __device__ __forceinline__ float4 philox_noise_pair(uint32_t key0, uint32_t key1
     return make_float4(g0.x, g0.y, g1.x, g1.y);
 }
 
+// One millisecond of noise for the nodes [r0, r0 + n_own) of a CTA, drawn by
+// the whole block into a ring stage laid out [substep][R] (float2 E, I); the
+// nodes at or above n_real (a padding node) get zeros.  The caller orders
+// the writes before the reads with a block barrier.
+__device__ __forceinline__ void philox_fill_stage(float2* stage, int R, int r0, int n_own, int n_real, int ms,
+                                                  uint32_t key0, uint32_t key1) {
+    for (int k = threadIdx.x; k < 5 * n_own; k += blockDim.x) {
+        const int pair = k / n_own, i = k - pair * n_own, node = r0 + i;
+        const float4 v = node < n_real ? philox_noise_pair(key0, key1, ms, pair, node, n_real)
+                                       : make_float4(0.f, 0.f, 0.f, 0.f);
+        stage[(2 * pair) * R + i] = make_float2(v.x, v.y);
+        stage[(2 * pair + 1) * R + i] = make_float2(v.z, v.w);
+    }
+}
+
 }  // namespace bnm

@@ -40,8 +40,8 @@ enum { BNM_PREC_F32 = 0, BNM_PREC_F64 = 1, BNM_PREC_F32_REF = 2 };
 
 /* Noise source.  PHILOX: counter-based Philox4x32-10 + Box-Muller keyed by
  * noise_seed, shared by all particles and FIC trials (the reference's
- * common-random-numbers semantics); the FP32 register integrator (N <= 128)
- * draws the values where it uses them (no table), the other kernels read a
+ * common-random-numbers semantics); the FP32 integrators draw the values
+ * where they use them (no table in HBM), the reference-order kernels read a
  * table of the same values.  HOST: the caller's precomputed table (the
  * reference's mt19937 + normal_distribution<float> stream,
  * run_CMAES.cpp:640-657). */
@@ -267,10 +267,10 @@ int bnm_plan_noise(bnm_plan *plan, int64_t offset, int64_t n, float *out);
  * Calls with fewer than 2 node pairs are rejected with BNM_EINVAL as well.
  * All calls share the array: the call zeroes what it accumulates, but calls
  * that overlap on the GPU race.  The first call on a device looks up the
- * array's address.  emp_fc and emp_fcd_sorted are copied to the device
- * asynchronously on the stream (usually from pageable memory, which the
- * runtime stages before the call returns); a call is not meant to be
- * recorded into a CUDA graph. */
+ * array's address.  emp_fc and emp_fcd_sorted are copied to the device on
+ * the stream: from pageable memory the runtime has staged them when the call
+ * returns; from page-locked memory the copy runs asynchronously, so keep them
+ * unchanged until the stream has passed the call. */
 #define BNM_NOALLOC_SCRATCH_BYTES ((size_t)32 << 20)
 int bnm_gof_noalloc(const float *d_bold, int32_t n, int32_t frames, int32_t nodes, int32_t n_vols_remove,
                     int32_t window_size, int32_t window_step, int32_t exc_interhem, int32_t use_fc_diff,
