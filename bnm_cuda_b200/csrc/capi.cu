@@ -262,19 +262,26 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
     BNM_CUDA_TRY(cudaMemcpy(p->d_sc64, sc, (size_t)N * N * 8, cudaMemcpyHostToDevice));
     BNM_CUDA_TRY(cudaMemcpy(p->d_sc_fic, scfic.data(), scfic.size() * 8, cudaMemcpyHostToDevice));
 
-    // noise: the caller's table, or Philox values drawn where they are consumed
-    // by the FP32 integrators (register kernel and both cluster kernels: no
-    // table at all), or a Philox table for the reference-order kernel, which
-    // reads one (also the FP32 path's only kernel where no cluster shape fits
-    // N; BNM_B200_NOISE_TABLE=1 forces the table for every kernel)
-    const char* nt = std::getenv("BNM_B200_NOISE_TABLE");
-    bool fp32_inline = cfg->precision == BNM_PREC_F32 && bnm_fast_kmax(N);
-    if (cfg->precision == BNM_PREC_F32 && !fp32_inline) {
+    // noise: the caller's table (HOST), or Philox values.  The FP32 kernels can
+    // draw those where they use them (no table): the cluster kernels (N > 128)
+    // do by default, one millisecond per block at a time; the register kernel
+    // (N <= 128) reads a table by default, because drawing in place lengthens
+    // its substep (measured at N = 100, 256 particles: 149.2 against 170.7
+    // sims/s).  The reference-order kernels always read a table.
+    // BNM_B200_NOISE_SOURCE=table|inline overrides the FP32 default.
+    bool can_inline = cfg->precision == BNM_PREC_F32 && bnm_fast_kmax(N);
+    if (cfg->precision == BNM_PREC_F32 && !can_inline) {
         IntegratorShape cand[128];
         const int nc = bnm_integrator_candidates(N, cand, 128);
-        for (int i = 0; i < nc; i++) fp32_inline |= cand[i].kind != 2;
+        for (int i = 0; i < nc; i++) can_inline |= cand[i].kind != 2;
     }
-    const bool table = cfg->noise_mode == BNM_NOISE_HOST || !fp32_inline || (nt && std::strcmp(nt, "0"));
+    bool inline_noise = can_inline && !bnm_fast_kmax(N);
+    if (const char* ns = std::getenv("BNM_B200_NOISE_SOURCE")) {
+        if (!std::strcmp(ns, "table")) inline_noise = false;
+        else if (!std::strcmp(ns, "inline")) inline_noise = can_inline;
+        else return fail(BNM_EINVAL, "BNM_B200_NOISE_SOURCE must be table or inline");
+    }
+    const bool table = cfg->noise_mode == BNM_NOISE_HOST || !inline_noise;
     p->noise_ld = N + p->pad;
     if (table) {
         const size_t rows = (size_t)(cfg->time_steps + 1) * 10;  // substeps; a row holds (E, I) of every node

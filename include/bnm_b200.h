@@ -40,9 +40,12 @@ enum { BNM_PREC_F32 = 0, BNM_PREC_F64 = 1, BNM_PREC_F32_REF = 2 };
 
 /* Noise source.  PHILOX: counter-based Philox4x32-10 + Box-Muller keyed by
  * noise_seed, shared by all particles and FIC trials (the reference's
- * common-random-numbers semantics); the FP32 integrators draw the values
- * where they use them (no table in HBM), the reference-order kernels read a
- * table of the same values.  HOST: the caller's precomputed table (the
+ * common-random-numbers semantics).  The FP32 cluster kernels (N > 128) draw
+ * the values where they use them (no table in HBM); the register kernel
+ * (N <= 128) and the reference-order kernels read a table of the same values
+ * (BNM_B200_NOISE_SOURCE=inline|table overrides the FP32 default; drawing in
+ * place lengthens the register kernel's substep).  HOST: the caller's
+ * precomputed table (the
  * reference's mt19937 + normal_distribution<float> stream,
  * run_CMAES.cpp:640-657). */
 enum { BNM_NOISE_PHILOX = 0, BNM_NOISE_HOST = 1 };

@@ -160,8 +160,8 @@ def test_autotuner_picks_a_timed_cluster_shape(cases):
 @pytest.mark.parametrize("N,shape", [(160, "3,10,2,4,10"), (160, "1,0,2,8,5"), (133, "4,10,2,4,10")])
 def test_cluster_kernels_draw_the_philox_table_values(N, shape, monkeypatch):
     """The cluster kernels draw their Philox noise by block, one millisecond at a
-    time, instead of copying it from a table; with the table forced
-    (BNM_B200_NOISE_TABLE=1) they stream the same values.  Results must be
+    time, instead of copying it from a table (their default); with the table
+    (BNM_B200_NOISE_SOURCE=table) they stream the same values.  Results must be
     bit-identical, row-split and column-split, odd N (padding node) included."""
     sc = synth.make_sc(N, 0.3, 7)
     G, wEE, wEI = synth.uniform_params(3, N, seed=21, g=(0.5, 2.0))
@@ -172,8 +172,8 @@ def test_cluster_kernels_draw_the_philox_table_values(N, shape, monkeypatch):
     emp_fc, emp_fcd = rng.uniform(-0.2, 0.8, s["n_pairs"]), rng.uniform(-0.3, 1.0, 200)
     monkeypatch.setenv("BNM_B200_SHAPE", shape)
     out = []
-    for table in ("0", "1"):
-        monkeypatch.setenv("BNM_B200_NOISE_TABLE", table)
+    for source in ("inline", "table"):
+        monkeypatch.setenv("BNM_B200_NOISE_SOURCE", source)
         with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
             out.append(p.run(G, wEE, wEI))
     for k in ("cost", "bold", "w_ie", "fic_penalty", "ext_means"):
