@@ -231,6 +231,24 @@ def cpu_reference_sample(n_threads: int, sample_ms: int = SAMPLE_MS, fp32: bool 
                         "sample_s": t_sample + t_gof, "per_sim_s": per_sim}
 
 
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "integrate_fast_kernel_N100_20s_x256_traffic.txt")
+
+
+def integrator_traffic() -> dict:
+    """roofline.traffic of the integrator: DRAM bytes (read + write) of one
+    launch from the committed ncu capture (a 20 s, 256-particle case of the
+    same kernel and noise source), scaled to this run's model time; null when
+    the summary is missing."""
+    try:
+        kv = dict(line.split(None, 1) for line in open(TRAFFIC_FILE) if line.strip() and not line.startswith("#"))
+        b, ms = float(kv["dram_bytes_per_launch"]), float(kv["model_ms"])
+    except (OSError, KeyError, ValueError):
+        return {"traffic": None, "traffic_source": "no committed capture"}
+    return {"traffic": b * (T_MS + 1) / (ms + 1),
+            "traffic_source": f"ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch at {int(ms)} ms model "
+                              f"time ({b / 1e6:.1f} MB), scaled to {T_MS} ms ({os.path.relpath(TRAFFIC_FILE, ROOT)})"}
+
+
 def workload_config(world: int = 1) -> dict:
     """The workload as both arms report it (same keys and values)."""
     return {"workload": WORKLOAD, "nodes": N_NODES, "particles_per_gpu": N_SIMS, "model_time_ms": T_MS,
@@ -371,10 +389,7 @@ def run_b200(args):
             "gpu_launches": launches,
             "roofline": {"bound": "fp32", "kernel": "integrate_fast_kernel", "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
-                         "traffic": 172.6e6 * (T_MS + 1) / 20001,
-                         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of this kernel on "
-                                           "the same workload at 20 s model time (172.6 MB), scaled by model "
-                                           "time (profiles/integrate_fast_kernel_N100_dram_traffic.md)",
+                         **integrator_traffic(),
                          "peak_source": "measured on this GPU by bnm_measure_fp32_peak (packed FP32 FMA chains)",
                          "work": "2*N^2 FLOP per substep per particle (coupling FMAs only), FIC restarts included"},
             "stage_ms": {k: float(v) for k, v in plan.timings().items()},

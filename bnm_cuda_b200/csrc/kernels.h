@@ -150,7 +150,8 @@ namespace bnm {
 // with `slots` particles per CTA; kind 1: row-split cluster kernel (N <= 512,
 // even) with `csize` CTAs per particle, `rpw` nodes per warp and `kr` SC
 // column chunks in registers; kind 2: the reference-order kernel in FP32 (any
-// N); kind 3: column-split cluster kernel (N <= 512, even) with `csize` CTAs
+// N); kind 3: column-split cluster kernel (N > 128, an odd N launched with one
+// padding node, up to the node count whose SC slice fits an SM) with `csize` CTAs
 // per particle, `slots` column pairs per warp, `rpw` rows per lane and `kr`
 // column pairs in registers; kind 4: column-split cluster kernel with two
 // particles per cluster (fields as kind 3).

@@ -207,9 +207,10 @@ int bnm_last_timings(bnm_plan *plan, double *ms6);
 
 /* FP32 integrator configuration the autotuner picked for the plan's last
  * batch size (no counterpart in the reference, which has one kernel shape).
- * out5: kind (0 register-SC kernel for N <= 128; 1 row-split and 3
- * column-split thread-block-cluster kernels for 128 < N <= 512, 4 the
- * column-split kernel with two particles per cluster; 2 reference-order
+ * out5: kind (0 register-SC kernel for N <= 128; 1 row-split
+ * thread-block-cluster kernel for even 128 < N <= 512; 3 column-split
+ * cluster kernel for N > 128 up to about 900 nodes, an odd N with one
+ * padding node; 4 the column-split kernel with two particles per cluster; 2 reference-order
  * kernel), then kind 0: particles per CTA; kind 1: -, CTAs per particle,
  * nodes per warp, SC column chunks of 32 in registers; kinds 3 and 4: column
  * pairs per warp, CTAs per cluster, rows per lane, column pairs in
