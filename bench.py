@@ -383,7 +383,8 @@ def run_b200(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": workload_config(world),
             "impl_config": {"precision": "f32 integration, f64 FIC/centring", "gram": args.gram,
-                            "integrator": plan.integrator(), "noise": "philox table"},
+                            "integrator": plan.integrator(), "window_tile": plan.window_tile(),
+                            "noise": "philox table", "graph_launched": plan.graph_launched()},
             "e2e": {"value": e2e, "unit": "sims/s", "h2d_bytes_per_step": 8 * (n + 2 * n * N),
                     "d2h_bytes_per_step": 8 * n * 5 + 4 * n * 3 + 8 * n * N},
             "gpu_launches": launches,

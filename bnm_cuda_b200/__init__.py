@@ -98,6 +98,7 @@ def lib():
         L.bnm_bw_math_probe.argtypes = [i32, vp, i32, vp]
         L.bnm_wait_probe.argtypes = [i32, C.c_int64, vp, vp]
         L.bnm_plan_graph.argtypes = [vp, vp]
+        L.bnm_plan_window_tile.argtypes = [vp, vp, vp]
         L.bnm_philox_probe.argtypes = [i32, vp, i32, vp]
         L.bnm_calculate_params.argtypes = [i32, i32, i32, vp, dbl, dbl, dbl, dbl, vp, vp, vp, vp, vp]
         L.bnm_gof_noalloc.argtypes = [vp, i32, i32, i32, i32, i32, i32, i32, i32, dbl, vp, i32, vp, i32, vp, vp]
@@ -275,6 +276,12 @@ class Plan:
         t, k = np.zeros(2), C.c_int32()
         _check(lib().bnm_last_gram(self._h, _ptr(t), C.byref(k)))
         return dict(fc_gram_ms=float(t[0]), fcd_gram_ms=float(t[1]), launches=k.value)
+
+    def window_tile(self) -> dict:
+        """Window-FC tile the tuner picked (pairs per thread of a 256-thread CTA)."""
+        t, k = C.c_int32(), C.c_int32()
+        _check(lib().bnm_plan_window_tile(self._h, C.byref(t), C.byref(k)))
+        return dict(pairs_per_thread=t.value, pairs_per_cta=256 * t.value, tried=k.value)
 
     def graph_launched(self) -> bool:
         """Whether the last run was one CUDA graph launch (bnm_plan_graph)."""

@@ -361,9 +361,9 @@ __global__ void __launch_bounds__(1024) gof_kernel(GofArgs a) {
 
 using namespace bnm;
 
-template <typename TB>
-static cudaError_t launch_fc_window(const FcArgs& a, const TB* bold, cudaStream_t st) {
-    constexpr int PPT = 4, TPB = 256;
+template <typename TB, int PPT>
+static cudaError_t launch_fc_window_t(const FcArgs& a, const TB* bold, cudaStream_t st) {
+    constexpr int TPB = 256;
     const int chunks = (a.P + TPB * PPT - 1) / (TPB * PPT);
     const size_t smem = (size_t)a.N * 5 * sizeof(double) + 2 * sizeof(double) + (size_t)a.win_len * a.N * sizeof(TB);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
@@ -372,6 +372,20 @@ static cudaError_t launch_fc_window(const FcArgs& a, const TB* bold, cudaStream_
     dim3 grid(a.n_sims, chunks);
     fc_window_kernel<TB, PPT><<<grid, TPB, smem, st>>>(a, bold);
     return cudaGetLastError();
+}
+
+// The window tile: each CTA of 256 threads carries 256 ppt pairs through the
+// frames (ppt in {1, 2, 4, 8}); fewer pairs per CTA give more CTAs but repeat
+// the node means and the frame ring per CTA.  The plan's tuner picks ppt.
+template <typename TB>
+static cudaError_t launch_fc_window(const FcArgs& a, const TB* bold, cudaStream_t st) {
+    switch (a.ppt ? a.ppt : 4) {
+        case 1: return launch_fc_window_t<TB, 1>(a, bold, st);
+        case 2: return launch_fc_window_t<TB, 2>(a, bold, st);
+        case 4: return launch_fc_window_t<TB, 4>(a, bold, st);
+        case 8: return launch_fc_window_t<TB, 8>(a, bold, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 
 cudaError_t bnm_launch_fc_window(const FcArgs& a, cudaStream_t st) {

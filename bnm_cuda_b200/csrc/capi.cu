@@ -175,6 +175,8 @@ struct bnm_plan {
     cudaGraph_t run_graph = nullptr;
     cudaGraphExec_t run_exec = nullptr;
     int run_graph_n = 0, last_graph = 0;
+    // window-FC tile (pairs per thread) picked by the tuner for batches of win_tuned_n particles
+    int win_ppt = 0, win_tuned_n = 0, win_tried = 0;
     double timings[6] = {0, 0, 0, 0, 0, 0};
     // tensor-core Gram kernels alone: one event pair per launch (FC, then each FCD chunk)
     std::vector<cudaEvent_t> gev;
@@ -586,16 +588,16 @@ static int ensure_hemi(bnm_plan* p) {
     return BNM_OK;
 }
 
-static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty, bool hemis = false) {
+static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty, bool hemis = false);
+
+// Window FC + static FC of the plan's BOLD buffer (fc_window_kernel).
+static FcArgs fc_args(bnm_plan* p, int n) {
     const bnm_config& c = p->cfg;
     const bnm_sizes& s = p->sz;
-    const int N = c.nodes;
-    cudaStream_t st = p->st;
-    p->n_gram = 0;
-    p->launches += 2;  // window FC and goodness of fit
-
     FcArgs fa;
-    fa.N = N;
+    std::memset(&fa, 0, sizeof fa);
+    fa.ppt = p->win_ppt;
+    fa.N = c.nodes;
     fa.n_sims = n;
     fa.frames = s.frames;
     fa.n_vols_remove = s.n_vols_remove;
@@ -612,7 +614,66 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty, bool hemis 
     fa.wfc = p->d_wfc;
     fa.wsum = p->d_wsum;
     fa.nan_flag = p->d_nan;
-    BNM_CUDA_TRY(bnm_launch_fc_window(fa, st));
+    return fa;
+}
+
+static int launch_window_only(bnm_plan* p, int n) {
+    BNM_CUDA_TRY(bnm_launch_fc_window(fc_args(p, n), p->st));
+    return BNM_OK;
+}
+
+// Window-tile tuner: times the window-FC kernel with 1, 2, 4 and 8 pairs per
+// thread (256, 512, 1024 and 2048 pairs per CTA) on this batch size and keeps
+// the fastest, on the first run of each batch size (BNM_B200_TUNE=0: 4).  The
+// timing launches accumulate into the window sums and NaN flags, which are
+// cleared afterwards.
+static int tune_window(bnm_plan* p, int n) {
+    if (p->win_tuned_n == n) return BNM_OK;
+    const char* tune = std::getenv("BNM_B200_TUNE");
+    p->win_ppt = 4;
+    p->win_tried = 0;
+    if (!(tune && std::atoi(tune) == 0)) {
+        double best = 1e300;
+        for (int ppt : {1, 2, 4, 8}) {
+            const int saved = p->win_ppt;
+            p->win_ppt = ppt;
+            float ms = 0.f;
+            bool ok = true;
+            for (int rep = 0; rep < 2 && ok; rep++) {  // the first launch also loads the kernel
+                BNM_CUDA_TRY(cudaEventRecord(p->tev[0], p->st));
+                const int launches = p->launches;
+                ok = launch_window_only(p, n) == BNM_OK;
+                p->launches = launches;
+                BNM_CUDA_TRY(cudaEventRecord(p->tev[1], p->st));
+            }
+            cudaGetLastError();  // a tile that cannot launch is skipped
+            BNM_CUDA_TRY(cudaStreamSynchronize(p->st));
+            if (!ok) {
+                p->win_ppt = saved;
+                continue;
+            }
+            BNM_CUDA_TRY(cudaEventElapsedTime(&ms, p->tev[0], p->tev[1]));
+            p->win_tried++;
+            if (ms < best) best = ms;
+            else p->win_ppt = saved;
+        }
+    }
+    const size_t W = std::max(p->sz.n_windows, 1);
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_wsum, 0, (size_t)n * W * 2 * 8, p->st));
+    BNM_CUDA_TRY(cudaMemsetAsync(p->d_nan, 0, n * 4, p->st));
+    p->win_tuned_n = n;
+    return BNM_OK;
+}
+
+static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty, bool hemis) {
+    const bnm_config& c = p->cfg;
+    const bnm_sizes& s = p->sz;
+    const int N = c.nodes;
+    cudaStream_t st = p->st;
+    p->n_gram = 0;
+    p->launches += 2;  // window FC and goodness of fit
+
+    BNM_CUDA_TRY(bnm_launch_fc_window(fc_args(p, n), st));
     const int split = c.gram == BNM_GRAM_BF16_SPLIT;
     if (c.gram != BNM_GRAM_F32) {
         // FC again as a tensor-core Gram; it replaces the co-moment FC in d_fc
@@ -949,7 +1010,8 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     const bool device_fic = c.do_fic && !w_ie;
     // after the first (tuning) run of a batch size, the generation is one graph launch
     const char* ge = std::getenv("BNM_B200_GRAPH");
-    if (device_fic && !hemis && c.precision == BNM_PREC_F32 && p->tuned_n == n && !(ge && !std::strcmp(ge, "0")))
+    if (device_fic && !hemis && c.precision == BNM_PREC_F32 && p->tuned_n == n && p->win_tuned_n == n &&
+        !(ge && !std::strcmp(ge, "0")))
         return run_graph(p, n, G, w_ee, w_ei, out);
     p->last_graph = 0;
     int rc = hemis ? ensure_hemi(p) : BNM_OK;
@@ -985,6 +1047,7 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     }
     else
         BNM_CUDA_TRY(bnm_launch_integrate_exact(a, c.precision == BNM_PREC_F64, p->num_sms, st));
+    if ((rc = tune_window(p, n))) return rc;
     BNM_CUDA_TRY(cudaEventRecord(p->ev[2], st));
     if ((rc = launch_analysis(p, n, c.calculate_fic_penalty, hemis))) return rc;
     return finish(p, n, out, true);
@@ -1016,6 +1079,8 @@ extern "C" int bnm_check_fit_bold(bnm_plan* p, int32_t n, const double* bold, bn
                                          per * 4, cudaMemcpyHostToDevice, st));
         BNM_CUDA_TRY(cudaStreamSynchronize(st));  // tmp goes out of scope
     }
+    int rc = tune_window(p, n);
+    if (rc) return rc;
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, st));
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_nan, 0, n * 4, st));
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_failed, 0, n * 4, st));
@@ -1026,7 +1091,7 @@ extern "C" int bnm_check_fit_bold(bnm_plan* p, int32_t n, const double* bold, bn
     for (int e = 0; e < 3; e++) BNM_CUDA_TRY(cudaEventRecord(p->ev[e], st));
     p->launches = 0;
     const bool hemis = out->fcd_left || out->fcd_right;
-    int rc = hemis ? ensure_hemi(p) : BNM_OK;
+    rc = hemis ? ensure_hemi(p) : BNM_OK;
     if (rc) return rc;
     rc = launch_analysis(p, n, 0, hemis);
     if (rc) return rc;
@@ -1274,6 +1339,7 @@ extern "C" int bnm_group_run(bnm_group* g, const int32_t* n, const double* const
                 if ((rc = launch_fic(p, sizes[i]))) return rc;
                 if ((rc = tune_integrator(p, sim_args(p, sizes[i]), np > 1))) return rc;
             }
+            if ((rc = tune_window(p, sizes[i]))) return rc;
         }
         BNM_CUDA_TRY(cudaEventRecord(g->t0, g->origin));
         BNM_CUDA_TRY(cudaEventRecord(g->fork, g->origin));
@@ -1335,6 +1401,13 @@ extern "C" int bnm_last_gram(bnm_plan* p, double* ms2, int32_t* launches) {
     ms2[0] = p->gram_ms[0];
     ms2[1] = p->gram_ms[1];
     if (launches) *launches = p->launches;
+    return BNM_OK;
+}
+
+extern "C" int bnm_plan_window_tile(bnm_plan* p, int32_t* pairs_per_thread, int32_t* n_tried) {
+    if (!p || !pairs_per_thread) return fail(BNM_EINVAL, "null argument");
+    *pairs_per_thread = p->win_ppt ? p->win_ppt : 4;
+    if (n_tried) *n_tried = p->win_tried;
     return BNM_OK;
 }
 

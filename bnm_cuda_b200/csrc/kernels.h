@@ -19,6 +19,7 @@ struct FcArgs {
     float* wfc;               // [n][W][P] raw window FC
     double* wsum;             // [n][W][2] sum, sum of squares over pairs (zeroed)
     int* nan_flag;            // [n]
+    int ppt;                  // pairs per thread: a CTA of 256 threads covers 256 ppt pairs (0: 4)
 };
 
 struct FcdArgs {

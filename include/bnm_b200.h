@@ -220,6 +220,14 @@ int bnm_last_timings(bnm_plan *plan, double *ms6);
  * shape and BNM_B200_TUNE=0 skips the timing. */
 int bnm_plan_integrator(bnm_plan *plan, int32_t *out5, int32_t *n_tried);
 
+/* Window-FC tile the tuner picked for the plan's last batch size (no
+ * counterpart in the reference, whose fc kernel covers maxThreadsPerBlock
+ * pairs per block, bnm.cu:649-708): *pairs_per_thread in {1, 2, 4, 8}, a CTA
+ * of 256 threads covering 256 x that many pairs; *n_tried: tiles timed.
+ * Tuned with the integrator on the first run of each batch size
+ * (BNM_B200_TUNE=0: 4, untimed). */
+int bnm_plan_window_tile(bnm_plan *plan, int32_t *pairs_per_thread, int32_t *n_tried);
+
 /* Measured FP32 FMA throughput of a device (packed fma.rn.f32x2 chains), in
  * TFLOP/s: the roofline denominator of the FP32-pipe-bound integrator.  No
  * counterpart in the reference. */

@@ -170,3 +170,28 @@ def test_hemisphere_fcd_against_fp64_oracle(case, port):
             right = port.port_fcd_tril(kept[:, h:], step, ws, exc=False)
             assert np.abs(r["fcd_left"][i] - left).max() <= 1e-4
             assert np.abs(r["fcd_right"][i] - right).max() <= 1e-4
+
+
+def test_window_tile_tuner_gives_the_same_window_fc(monkeypatch):
+    """The window-FC tile (pairs per CTA) is tuned on the first run of a batch
+    size; every tile computes the same window FC (each pair's co-moments are
+    formed by one thread whatever the tile), so the tuned plan and plans forced
+    to the default tile must agree on FC and FCD."""
+    N = 40
+    sc = synth.make_sc(N, 0.3, 2)
+    cfg = B.Config(nodes=N, max_sims=4, time_steps=30000, bold_tr=500, window_size=10, window_step=2,
+                   bold_remove_s=2, gram=B.GRAM_F32)
+    s = cfg.sizes()
+    rng = np.random.default_rng(4)
+    emp_fc, emp_fcd = rng.uniform(-0.2, 0.8, s["n_pairs"]), rng.uniform(-0.3, 1.0, 300)
+    G, wEE, wEI = synth.uniform_params(4, N, 8)
+    with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+        a = p.run(G, wEE, wEI)
+        tile = p.window_tile()
+    assert tile["tried"] == 4 and tile["pairs_per_thread"] in (1, 2, 4, 8), tile
+    monkeypatch.setenv("BNM_B200_TUNE", "0")
+    with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+        b = p.run(G, wEE, wEI)
+        assert p.window_tile()["pairs_per_thread"] == 4
+    np.testing.assert_array_equal(a["fc"], b["fc"])
+    np.testing.assert_allclose(a["fcd"], b["fcd"], rtol=0, atol=1e-6)
