@@ -452,7 +452,7 @@ def run_surrogate(args):
             plain = S.run_cmaes(plan, bounds, 64, args.generations, seed=seed)
             mlp.set_params(trained)
             screen = S.run_cmaes(plan, bounds, 64, args.generations, seed=seed, mlp=mlp, spec=spec, oversample=8,
-                                 holdout_rmse=info["holdout_rmse"])
+                                 holdout_spearman=info["holdout_spearman"])
             target = min(plain["best"], screen["best"]) + 0.01
             tp_, ts_ = to_target(plain, target), to_target(screen, target)
             seeds.append({"seed": seed, "plain_best": plain["best"], "screened_best": screen["best"],

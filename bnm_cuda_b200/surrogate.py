@@ -8,8 +8,11 @@ distance, FIC penalty).  Screened CMA-ES draws ``oversample`` x lambda
 candidates per generation from the current search distribution, ranks them
 by predicted cost and injects the best lambda as the generation's samples;
 only simulated costs reach the optimiser.  Every reported fit is a simulated
-one, and the screening is switched off (plain CMA-ES) when the surrogate's
-held-out error exceeds a threshold.
+one.  Screening uses only the ranking of candidates, so the surrogate is
+trusted when it ranks held-out simulations well (Spearman correlation of
+predicted and simulated cost at least ``min_rank_corr``) and screening is
+switched off (plain CMA-ES) otherwise, or once its error on the simulated
+candidates exceeds their spread two generations running.
 """
 from __future__ import annotations
 
@@ -190,10 +193,10 @@ def train_surrogate(plan: Plan, bounds: Bounds, spec: np.ndarray, n_train: int, 
 
 
 def run_cmaes(plan: Plan, bounds: Bounds, lam: int, generations: int, seed: int, mlp: MLP | None = None,
-              spec: np.ndarray | None = None, oversample: int = 8, threshold: float = 0.1,
-              holdout_rmse: float | None = None, cand_seed: int = 12345, replay: int = 1024):
+              spec: np.ndarray | None = None, oversample: int = 8, min_rank_corr: float = 0.9,
+              holdout_spearman: float | None = None, cand_seed: int = 12345, replay: int = 1024):
     """Plain CMA-ES, or surrogate-pre-screened CMA-ES when an MLP is given and
-    its held-out RMSE is within ``threshold``.
+    its held-out rank correlation is at least ``min_rank_corr``.
 
     Screening: each generation draws oversample*lambda candidates from the
     current N(m, sigma^2 C), keeps the lambda with the lowest predicted cost,
@@ -204,7 +207,7 @@ def run_cmaes(plan: Plan, bounds: Bounds, lam: int, generations: int, seed: int,
     stops for good once the surrogate no longer separates the candidates: its
     error on the simulated ones exceeds their spread two generations in a
     row.  Returns the best simulated cost and wall time per generation."""
-    screened = mlp is not None and (holdout_rmse is None or holdout_rmse <= threshold)
+    screened = mlp is not None and (holdout_spearman is None or holdout_spearman >= min_rank_corr)
     es = CMAES(lam, 3, seed, generations + 1, from_env=False)
     rng = np.random.default_rng(cand_seed)
     best, best_x, hist, walls, errs, spreads, bad = np.inf, None, [], [], [], [], 0

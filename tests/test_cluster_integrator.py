@@ -66,7 +66,7 @@ SHAPES = {
 # kernels, N = 130 and 512)
 SHAPES["n130"] = ["auto"]
 SHAPES["n512"] = ["auto"]
-SHAPES["n133"] = ["auto", "3,10,1,5,10", "4,10,2,4,10"]
+SHAPES["n133"] = ["auto", "3,10,1,5,10", "4,13,2,4,13"]  # 134 columns: 6 warps of 2 x 13 pairs
 SHAPES["n379"] = ["auto", "4,25,4,4,20"]
 SHAPES["n600"] = ["auto"]
 KINDS = {0: "register", 1: "cluster", 3: "colsplit", 4: "colsplit2"}
@@ -157,7 +157,7 @@ def test_autotuner_picks_a_timed_cluster_shape(cases):
     np.testing.assert_array_equal(r1["cost"], r2["cost"])
 
 
-@pytest.mark.parametrize("N,shape", [(160, "3,10,2,4,10"), (160, "1,0,2,8,5"), (133, "4,10,2,4,10")])
+@pytest.mark.parametrize("N,shape", [(160, "3,10,2,4,10"), (160, "1,0,2,8,5"), (133, "4,13,2,4,13")])
 def test_cluster_kernels_draw_the_philox_table_values(N, shape, monkeypatch):
     """The cluster kernels draw their Philox noise by block, one millisecond at a
     time, instead of copying it from a table (their default); with the table
