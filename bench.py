@@ -49,6 +49,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 N_NODES, N_SIMS, T_MS, TR, WS, STEP, REMOVE_S = 100, 256, 450_000, 720, 44, 1, 30
+DEFAULT_SIMS, DEFAULT_T_MS = N_SIMS, T_MS
 SAMPLE_MS = 12_000
 WORKLOAD = "cmaes-generation-N100-450s-x256"
 
@@ -526,7 +527,10 @@ def run_precision(args):
     import bnm_cuda_b200 as B
     from bnm_cuda_b200 import synth
 
-    N, n, T, TRp, WSp, STEPp = 400, args.particles if args.particles != N_SIMS else 64, 600_000, 500, 44, 1
+    # --particles / --model-ms (profiling knobs) replace the 64 particles and 600 s when given
+    n = args.particles if args.particles != DEFAULT_SIMS else 64
+    T = args.model_ms if args.model_ms != DEFAULT_T_MS else 600_000
+    N, TRp, WSp, STEPp = 400, 500, 44, 1
     sc = synth.make_sc(N, 0.1, 0)
     G, wEE, wEI = synth.uniform_params(n, N, 1)
     cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TRp, window_size=WSp, window_step=STEPp,
@@ -578,7 +582,7 @@ def run_precision(args):
     print(json.dumps({
         "metric": "sims/s", "value": n / (tm["total"] / 1e3), "unit": "sims/s", "n_gpus": 1, "steps": 1,
         "higher_is_better": True, "data": "synthetic", "dtype": "f32 integration; FC/FCD Grams f32 / bf16 / bf16x3",
-        "config": {"workload": "precision-stress-N400-600s-x64", "nodes": N, "particles": n, "model_time_ms": T,
+        "config": {"workload": f"precision-stress-N400-{T // 1000}s-x{n}", "nodes": N, "particles": n, "model_time_ms": T,
                    "tr_ms": TRp, "window": WSp, "step": STEPp, "windows": W, "pairs": P, "fcd_entries": s["n_fcd"],
                    "sc_density": 0.1, "integrator": integ, "checked_particles": k},
         "wall_s": wall, "stage_ms": tm, "precision": table,
@@ -679,8 +683,10 @@ def main():
     ap.add_argument("--generations", type=int, default=60)
     ap.add_argument("--surrogate-seeds", type=int, default=5, help="surrogate: CMA-ES seeds compared")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU-baseline sample")
-    ap.add_argument("--particles", type=int, default=N_SIMS, help="profiling knob: particles per GPU")
-    ap.add_argument("--model-ms", type=int, default=T_MS, help="profiling knob: model time per simulation")
+    ap.add_argument("--particles", type=int, default=N_SIMS,
+                    help="profiling knob: particles per GPU (precision workload: particles, default 64)")
+    ap.add_argument("--model-ms", type=int, default=T_MS,
+                    help="profiling knob: model time per simulation (precision workload: default 600000)")
     ap.add_argument("--profile", action="store_true",
                     help="profiling knob: no integrator autotuning (BNM_B200_TUNE=0: the default shape, no timing "
                          "launches), so that a run's launch order is fixed: the target simulation's kernels, then "
