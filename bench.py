@@ -421,11 +421,14 @@ def run_surrogate(args):
     runs sample 8x lambda and simulate the best lambda by predicted cost.
 
     Over --surrogate-seeds CMA-ES seeds (each screened run starts from the
-    same trained network), like for like: the target of a seed is the better
-    of the two runs' final bests plus 0.01, and each run's time-to-target is
-    its wall time until its best is within that target.  Reported per seed
-    and as the median ratio screened / plain, without and with the surrogate's
-    one-off cost (training simulations + fit) added to the screened run."""
+    same trained network), like for like: the target of a seed is the plain
+    run's final best plus 0.01, and each run's time-to-target is its wall time
+    until its best is at or below that target (for the plain run, its own
+    time to come within 0.01 of its final best, not its whole run).  Reported
+    per seed (also against the better of the two final bests) and as the
+    median ratio screened / plain, without and with the surrogate's one-off
+    cost (training simulations + fit) added to the screened run; a screened
+    run that never reaches the target counts as +inf."""
     import bnm_cuda_b200 as B
     from bnm_cuda_b200 import surrogate as S, synth
 
@@ -454,29 +457,38 @@ def run_surrogate(args):
             mlp.set_params(trained)
             screen = S.run_cmaes(plan, bounds, 64, args.generations, seed=seed, mlp=mlp, spec=spec, oversample=8,
                                  holdout_spearman=info["holdout_spearman"])
-            target = min(plain["best"], screen["best"]) + 0.01
+            # the north star's target: within 0.01 of plain CMA-ES's final best
+            target = plain["best"] + 0.01
             tp_, ts_ = to_target(plain, target), to_target(screen, target)
+            # and the better of the two final bests + 0.01: a run that never gets there loses outright
+            better = min(plain["best"], screen["best"]) + 0.01
+            bp, bs = to_target(plain, better), to_target(screen, better)
             seeds.append({"seed": seed, "plain_best": plain["best"], "screened_best": screen["best"],
                           "target": target, "plain_time_s": tp_, "screened_time_s": ts_,
+                          "ratio": ts_ / tp_ if ts_ is not None else None,
+                          "ratio_with_training": (ts_ + t_surrogate) / tp_ if ts_ is not None else None,
+                          "better_target": better, "plain_time_to_better_s": bp, "screened_time_to_better_s": bs,
                           "plain_wall_s": plain["wall_hist"][-1], "screened_wall_s": screen["wall_hist"][-1],
-                          "ratio": ts_ / tp_ if tp_ and ts_ is not None else None,
-                          "ratio_with_training": (ts_ + t_surrogate) / tp_ if tp_ and ts_ is not None else None,
-                          "screened_within_001_of_plain": screen["best"] <= plain["best"] + 0.01,
                           "screened_generations": screen["screened_generations"],
                           "plain_hist": [round(b, 4) for b in plain["best_hist"]],
-                          "screened_hist": [round(b, 4) for b in screen["best_hist"]]})
-    ratios = [r["ratio"] for r in seeds if r["ratio"] is not None]
-    ratios_t = [r["ratio_with_training"] for r in seeds if r["ratio_with_training"] is not None]
+                          "screened_hist": [round(b, 4) for b in screen["best_hist"]],
+                          "plain_walls": [round(w, 3) for w in plain["wall_hist"]],
+                          "screened_walls": [round(w, 3) for w in screen["wall_hist"]]})
+    # a seed whose screened run never comes within 0.01 of plain's best counts as a loss (ratio +inf)
+    r_all = [r["ratio"] if r["ratio"] is not None else float("inf") for r in seeds]
+    r_all_t = [r["ratio_with_training"] if r["ratio_with_training"] is not None else float("inf") for r in seeds]
+    med, med_t = float(np.median(r_all)), float(np.median(r_all_t))
     print(json.dumps({
-        "metric": "CMA-ES time-to-target, surrogate-screened / plain (median over seeds)",
-        "value": float(np.median(ratios)) if ratios else None, "unit": "fraction of plain time-to-target",
-        "value_with_training": float(np.median(ratios_t)) if ratios_t else None,
+        "metric": "CMA-ES time to within 0.01 of plain's final best, surrogate-screened / plain (median over seeds)",
+        "value": med if np.isfinite(med) else None, "unit": "fraction of plain time-to-target",
+        "value_with_training": med_t if np.isfinite(med_t) else None,
+        "screened_reached_target": sum(r["ratio"] is not None for r in seeds), "seeds_run": len(seeds),
         "higher_is_better": False, "data": "synthetic",
         "config": {"workload": "cmaes-surrogate-N100-300s-lambda64x8", "train_sims": args.train_sims,
                    "generations": args.generations, "seeds": args.surrogate_seeds,
-                   "target": "better final best of the two runs + 0.01, per seed"},
+                   "target": "plain CMA-ES final best + 0.01, per seed (time of the first generation at or "
+                             "below it; a screened run that never gets there counts as +inf)"},
         "seeds": seeds, "surrogate_one_off_s": t_surrogate,
-        "screened_within_001_all": all(r["screened_within_001_of_plain"] for r in seeds),
         "surrogate": {k: v for k, v in info.items() if k != "losses"},
     }))
     return 0
