@@ -232,12 +232,12 @@ def cpu_reference_sample(n_threads: int, sample_ms: int = SAMPLE_MS, fp32: bool 
                         "sample_s": t_sample + t_gof, "per_sim_s": per_sim}
 
 
-TRAFFIC_FILE = os.path.join(ROOT, "profiles", "integrate_fast_kernel_N100_20s_x256_traffic.txt")
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "integrate_fast_kernel_N100_70s_x256_traffic.txt")
 
 
 def integrator_traffic() -> dict:
     """roofline.traffic of the integrator: DRAM bytes (read + write) of one
-    launch from the committed ncu capture (a 20 s, 256-particle case of the
+    launch from the committed ncu capture (a 70 s, 256-particle case of the
     same kernel and noise source), scaled to this run's model time; null when
     the summary is missing."""
     try:
