@@ -62,6 +62,7 @@ struct SimArgs {
     int* failed;        // [n]
     double* ext;        // [n][6][N] means of S_E, I_E, r_E, S_I, I_I, r_I over kept frames
     int* work_counter;  // persistent scheduling (zeroed before launch)
+    const int* order;   // optional placement: CTA b's first particle is order[b], later claims order[grid + k]
     int* status;
 };
 

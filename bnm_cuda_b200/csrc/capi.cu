@@ -177,6 +177,14 @@ struct bnm_plan {
     int run_graph_n = 0, last_graph = 0;
     // window-FC tile (pairs per thread) picked by the tuner for batches of win_tuned_n particles
     int win_ppt = 0, win_tuned_n = 0, win_tried = 0;
+    // placement of particles on the register kernel's CTAs by predicted FIC work (BNM_B200_PLACE=1):
+    // the parameters and FIC restart counts of the particles simulated so far
+    bool place = false;
+    int* d_order = nullptr;
+    int* io_order = nullptr;  // pinned [max_sims]
+    std::vector<float> hist_x;  // G, mean wEE, mean wEI per simulated particle
+    std::vector<int> hist_tr;
+    size_t hist_next = 0;
     double timings[6] = {0, 0, 0, 0, 0, 0};
     // tensor-core Gram kernels alone: one event pair per launch (FC, then each FCD chunk)
     std::vector<cudaEvent_t> gev;
@@ -200,6 +208,7 @@ extern "C" void bnm_plan_destroy(bnm_plan* p) {
     if (p->run_exec) cudaGraphExecDestroy(p->run_exec);
     if (p->run_graph) cudaGraphDestroy(p->run_graph);
     if (p->pinned) cudaFreeHost(p->pinned);
+    if (p->io_order) cudaFreeHost(p->io_order);
     for (auto& e : p->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : p->tev)
@@ -295,6 +304,17 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
         else
             BNM_CUDA_TRY(bnm_launch_philox(p->d_noise, (uint64_t)s.noise_len, N, p->noise_ld, cfg->noise_seed,
                                            p->num_sms, p->st));
+    }
+
+    // particle placement (register kernel, numerical FIC; opt-in)
+    if (const char* pl = std::getenv("BNM_B200_PLACE"))
+        p->place = !std::strcmp(pl, "1") && cfg->precision == BNM_PREC_F32 && p->kmax && cfg->do_fic &&
+                   cfg->numerical_fic;
+    if (p->place) {
+        BNM_CUDA_TRY(dalloc(p, &p->d_order, (size_t)cfg->max_sims));
+        BNM_CUDA_TRY(cudaMallocHost((void**)&p->io_order, (size_t)cfg->max_sims * sizeof(int)));
+        for (int i = 0; i < cfg->max_sims; i++) p->io_order[i] = i;
+        BNM_CUDA_TRY(cudaMemcpy(p->d_order, p->io_order, (size_t)cfg->max_sims * 4, cudaMemcpyHostToDevice));
     }
 
     // pair table (run_CMAES.cpp:505-524)
@@ -903,6 +923,7 @@ static SimArgs sim_args(bnm_plan* p, int n) {
     a.wEE = p->d_wEE;
     a.wEI = p->d_wEI;
     a.wIE = p->d_wIE;
+    a.order = p->place ? p->d_order : nullptr;
     a.noise = p->d_noise;  // NULL: the register integrator draws Philox noise in place
     a.noise_seed = c.noise_seed;
     a.noise_ld = p->noise_ld;
@@ -924,6 +945,92 @@ static SimArgs sim_args(bnm_plan* p, int n) {
 static int ensure_pinned(bnm_plan* p);
 static int enqueue_run(bnm_plan* p, int n);
 static int read_timings(bnm_plan* p);
+
+// Particle placement on the register kernel's CTAs (BNM_B200_PLACE=1).  A
+// particle that hits the numerical-FIC trial cap integrates about 1 M more
+// substeps than one that needs no restart, and with more particles than SMs
+// the CTAs share SMs (two per SM, each slower than alone), so the generation
+// ends with the heavy particles that shared an SM.  CTA b starts with the
+// particle at position b of io_order; the first num_sms CTAs go to distinct
+// SMs and CTA num_sms + k joins CTA k's SM, so positions [n - S, S) run alone.
+// Work is predicted by the FIC restart count of the nearest particle simulated
+// before by this plan (G, mean wEE, mean wEI, each scaled by its spread); the
+// heaviest take the lone positions, the others pair heaviest with lightest.
+// Without history the order is the identity.
+static void place_particles(bnm_plan* p, int n, const double* G, const double* w_ee, const double* w_ei) {
+    const int N = p->cfg.nodes, S = p->num_sms;
+    for (int i = 0; i < n; i++) p->io_order[i] = i;
+    const size_t H = p->hist_tr.size();
+    if (H < 16 || n <= 1) return;
+    double mu[3] = {0, 0, 0}, sd[3] = {0, 0, 0};
+    for (size_t h = 0; h < H; h++)
+        for (int d = 0; d < 3; d++) mu[d] += p->hist_x[3 * h + d];
+    for (int d = 0; d < 3; d++) mu[d] /= H;
+    for (size_t h = 0; h < H; h++)
+        for (int d = 0; d < 3; d++) sd[d] += (p->hist_x[3 * h + d] - mu[d]) * (p->hist_x[3 * h + d] - mu[d]);
+    for (int d = 0; d < 3; d++) sd[d] = sd[d] > 0 ? std::sqrt(sd[d] / H) : 1.0;
+    std::vector<int> pred(n);
+    for (int i = 0; i < n; i++) {
+        double x[3] = {G[i], 0, 0};
+        for (int j = 0; j < N; j++) {
+            x[1] += w_ee[(size_t)i * N + j];
+            x[2] += w_ei[(size_t)i * N + j];
+        }
+        x[1] /= N;
+        x[2] /= N;
+        double best = 1e300;
+        for (size_t h = 0; h < H; h++) {
+            double d2 = 0;
+            for (int d = 0; d < 3; d++) {
+                const double t = (x[d] - p->hist_x[3 * h + d]) / sd[d];
+                d2 += t * t;
+            }
+            if (d2 < best) {
+                best = d2;
+                pred[i] = p->hist_tr[h];
+            }
+        }
+    }
+    std::vector<int> by(n);
+    for (int i = 0; i < n; i++) by[i] = i;
+    std::stable_sort(by.begin(), by.end(), [&](int a, int b) { return pred[a] > pred[b]; });
+    if (n <= S || n > 2 * S) {  // every CTA alone, or more particles than CTAs: heaviest first
+        for (int i = 0; i < n; i++) p->io_order[i] = by[i];
+        return;
+    }
+    const int pairs = n - S, lone = S - pairs;
+    for (int k = 0; k < lone; k++) p->io_order[pairs + k] = by[k];
+    const int* rest = by.data() + lone;  // 2 * pairs particles, heaviest first
+    for (int k = 0; k < pairs; k++) {
+        p->io_order[k] = rest[k];
+        p->io_order[S + k] = rest[2 * pairs - 1 - k];
+    }
+}
+
+// Appends the last batch's particles and FIC restart counts to the placement history.
+static void record_particles(bnm_plan* p, int n, const double* G, const double* w_ee, const double* w_ei,
+                             const int* trials) {
+    const int N = p->cfg.nodes;
+    const size_t cap = 1 << 14;
+    for (int i = 0; i < n; i++) {
+        float x[3] = {(float)G[i], 0.f, 0.f};
+        double e = 0, f = 0;
+        for (int j = 0; j < N; j++) {
+            e += w_ee[(size_t)i * N + j];
+            f += w_ei[(size_t)i * N + j];
+        }
+        x[1] = (float)(e / N);
+        x[2] = (float)(f / N);
+        if (p->hist_tr.size() < cap) {
+            p->hist_x.insert(p->hist_x.end(), x, x + 3);
+            p->hist_tr.push_back(trials[i]);
+        } else {
+            const size_t h = p->hist_next++ % cap;
+            std::copy(x, x + 3, p->hist_x.begin() + 3 * h);
+            p->hist_tr[h] = trials[i];
+        }
+    }
+}
 
 // A generation of a plan whose integrator is already tuned for n particles,
 // with analytic FIC on the device: parameters staged through pinned host
@@ -948,6 +1055,7 @@ static int run_graph(bnm_plan* p, int n, const double* G, const double* w_ee, co
         p->io_wEE[i] = w_ee[i];
         p->io_wEI[i] = w_ei[i];
     }
+    if (p->place) place_particles(p, n, G, w_ee, w_ei);
     cudaStream_t st = p->st;
     if (!p->run_exec || p->run_graph_n != n) {
         if (p->run_exec) cudaGraphExecDestroy(p->run_exec);
@@ -994,6 +1102,7 @@ static int run_graph(bnm_plan* p, int n, const double* G, const double* w_ee, co
     put(out->fic_failed, p->io_failed, n);
     put(out->fic_ntrials, p->io_trials, n);
     put(out->fic_unstable, p->io_unstable, n);
+    if (p->place) record_particles(p, n, G, w_ee, w_ei, p->io_trials);
     return BNM_OK;
 }
 
@@ -1043,6 +1152,11 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
         if ((rc = tune_integrator(p, a))) return rc;
         BNM_CUDA_TRY(cudaMemsetAsync(p->d_counter, 0, 16, st));
         BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, st));
+        if (p->place) {
+            BNM_CUDA_TRY(cudaStreamSynchronize(st));  // the tuner's launches may still read the order
+            place_particles(p, n, G, w_ee, w_ei);
+            BNM_CUDA_TRY(cudaMemcpyAsync(p->d_order, p->io_order, n * 4, cudaMemcpyHostToDevice, st));
+        }
         BNM_CUDA_TRY(bnm_launch_integrate_shape(a, p->shape, p->num_sms, st));
     }
     else
@@ -1050,7 +1164,13 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
     if ((rc = tune_window(p, n))) return rc;
     BNM_CUDA_TRY(cudaEventRecord(p->ev[2], st));
     if ((rc = launch_analysis(p, n, c.calculate_fic_penalty, hemis))) return rc;
-    return finish(p, n, out, true);
+    rc = finish(p, n, out, true);
+    if (!rc && p->place) {
+        std::vector<int> tr(n);
+        BNM_CUDA_TRY(cudaMemcpy(tr.data(), p->d_trials, n * 4, cudaMemcpyDeviceToHost));
+        record_particles(p, n, G, w_ee, w_ei, tr.data());
+    }
+    return rc;
 }
 
 // Goodness of fit of given BOLD series (check_fit_bold, check_fit.cpp:138-217,
@@ -1151,6 +1271,7 @@ static int enqueue_run(bnm_plan* p, int n) {
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_hist, 0, (size_t)n * (p->m + 1) * 4, st));
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_eq, 0, (size_t)n * (p->m + 1) * 4, st));
     const SimArgs a = sim_args(p, n);
+    if (p->place) BNM_CUDA_TRY(cudaMemcpyAsync(p->d_order, p->io_order, n * 4, cudaMemcpyHostToDevice, st));
     if (c.precision == BNM_PREC_F32)
         BNM_CUDA_TRY(bnm_launch_integrate_shape(a, p->shape, p->num_sms, st));
     else

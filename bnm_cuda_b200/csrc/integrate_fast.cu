@@ -166,8 +166,16 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
         }
     };
     // take the next particle of the batch into slot p (all threads)
-    auto load = [&](int p) {
-        if (threadIdx.x == 0) s_sim[p] = atomicAdd(a.work_counter, 1);
+    // With a placement order (one particle per CTA only) CTA b starts with the
+    // particle the host put at position b and later claims continue after the
+    // grid; without one, particles go out in claim order.
+    const bool placed = P == 1 && a.order != nullptr;
+    auto load = [&](int p, bool initial) {
+        if (threadIdx.x == 0) {
+            const int c = placed && initial ? (int)blockIdx.x
+                                            : atomicAdd(a.work_counter, 1) + (placed ? (int)gridDim.x : 0);
+            s_sim[p] = c < a.n_sims ? (placed ? a.order[c] : c) : a.n_sims;
+        }
         __syncthreads();
         sim[p] = s_sim[p];
         live[p] = sim[p] < a.n_sims;
@@ -202,7 +210,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
 #pragma unroll
     for (int p = 0; p < P; p++) {
         c_cons[p] = c_issue[p] = 0;
-        load(p);
+        load(p, true);
     }
     int cur = 0;
 
@@ -452,7 +460,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
                     a.trials[sim[p]] = trial[p];
                     a.failed[sim[p]] = failed[p] ? 1 : 0;
                 }
-                load(p);
+                load(p, false);
             }
         }
         if (timed_out) break;
