@@ -148,7 +148,12 @@ def test_particle_placement_keeps_every_particles_result(monkeypatch):
         ref = [p.run(*P1), p.run(*P2)]
     monkeypatch.setenv("BNM_B200_PLACE", "1")
     with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
-        got = [p.run(*P1), p.run(*P2), p.run(*P2)]  # identity, then placed (eager), then placed (graph)
+        got = [p.run(*P1)]  # no history yet: identity order
+        monkeypatch.setenv("BNM_B200_GRAPH", "0")
+        got.append(p.run(*P2))  # placed, eager
+        assert not p.graph_launched()
+        monkeypatch.delenv("BNM_B200_GRAPH")
+        got.append(p.run(*P2))  # placed, graph launch
         assert p.graph_launched()
     for a, b in ((ref[0], got[0]), (ref[1], got[1]), (ref[1], got[2])):
         _same(a, b)
