@@ -54,14 +54,23 @@ SAMPLE_MS = 12_000
 WORKLOAD = "cmaes-generation-N100-450s-x256"
 
 
-def workload_inputs(world: int = 1):
+def workload_inputs(world: int = 1, seed: int = 1):
     """SC and the whole population: N_SIMS particles per rank (weak scaling);
-    rank r simulates particles [r N_SIMS, (r+1) N_SIMS) (bnm_cuda_b200.shard)."""
+    rank r simulates particles [r N_SIMS, (r+1) N_SIMS) (bnm_cuda_b200.shard).
+    The particles are a uniform draw on the parameter bounds (seed 1: the
+    first timed generation and the CPU reference's particles)."""
     from bnm_cuda_b200 import synth
 
     sc = synth.make_sc(N_NODES, 0.3, 0)
-    G, wEE, wEI = synth.uniform_params(N_SIMS * world, N_NODES, 1)
+    G, wEE, wEI = synth.uniform_params(N_SIMS * world, N_NODES, seed)
     return sc, G, wEE, wEI
+
+
+def generation_seeds(warmup: int, steps: int):
+    """Particle seeds of the warm-up and timed generations: every generation
+    draws new particles (as CMA-ES does), so the plan's placement history never
+    holds the particles it places."""
+    return [1001 + w for w in range(warmup)], [1 + k for k in range(steps)]
 
 
 def make_targets(sc):
@@ -254,6 +263,8 @@ def workload_config(world: int = 1) -> dict:
     """The workload as both arms report it (same keys and values)."""
     return {"workload": WORKLOAD, "nodes": N_NODES, "particles_per_gpu": N_SIMS, "model_time_ms": T_MS,
             "tr_ms": TR, "window": WS, "step": STEP, "fic": "analytic + numerical, up to 10 restarts",
+            "particles": "uniform on the parameter bounds, a fresh draw every generation (timed: seeds 1, 2, ...; "
+                         "warm-up: 1001, ...)",
             "l2": "inputs larger than L2 (3.6 GB noise stream, 1.4 GB window FC per generation)",
             "parallelism": f"particles sharded over {world} GPU(s)"}
 
@@ -324,17 +335,19 @@ def run_b200(args):
 
     from bnm_cuda_b200 import shard
 
-    sc, G_all, wEE_all, wEI_all = workload_inputs(world)
-    a, b = shard.shard_bounds(len(G_all), world, rank)
-    G, wEE, wEI = G_all[a:b], wEE_all[a:b], wEI_all[a:b]
+    warm_seeds, step_seeds = generation_seeds(args.warmup, args.steps)
+    sc = workload_inputs(world)[0]
+    gens = {k: workload_inputs(world, k)[1:] for k in warm_seeds + step_seeds}  # host arrays, made before timing
+    a, b = shard.shard_bounds(N_SIMS * world, world, rank)
     emp_fc, emp_fcd = make_targets(sc)
     gram = {"f32": B.GRAM_F32, "bf16": B.GRAM_BF16, "bf16x3": B.GRAM_BF16_SPLIT}[args.gram]
     cfg = B.Config(nodes=N_NODES, max_sims=N_SIMS, time_steps=T_MS, bold_tr=TR, window_size=WS, window_step=STEP,
                    bold_remove_s=REMOVE_S, noise_seed=410, device=local, gram=gram)
     plan = B.Plan(cfg, sc, emp_fc, emp_fcd)
     outputs = ("w_ie",)  # the reference returns corr, fic_penalties, w_IE_fic, FIC_failed, fic_n_trials
-    for _ in range(args.warmup):
-        plan.run(G, wEE, wEI, outputs=outputs)
+    for k in warm_seeds:
+        G_all, wEE_all, wEI_all = gens[k]
+        plan.run(G_all[a:b], wEE_all[a:b], wEI_all[a:b], outputs=outputs)
 
     def barrier():
         if dist:
@@ -343,18 +356,20 @@ def run_b200(args):
             dist.barrier()
 
     barrier()
-    dev_ms, integ_ms, wall, flops, launches = [], [], [], [], 0
+    dev_ms, integ_ms, wall, flops, launches, placed = [], [], [], [], 0, 0
     with ClockSampler(local) as clk:
-        for _ in range(args.steps):
+        for k in step_seeds:
+            G_all, wEE_all, wEI_all = gens[k]
             t0 = time.perf_counter()
             if dist:  # this rank's shard, then every particle's fit terms on every rank (NCCL)
                 r = shard.run_sharded(lambda g, e, i: plan.run(g, e, i, outputs=outputs), G_all, wEE_all, wEI_all)
                 torch.cuda.synchronize()
             else:
-                r = plan.run(G, wEE, wEI, outputs=outputs)
+                r = plan.run(G_all, wEE_all, wEI_all, outputs=outputs)
             wall.append(time.perf_counter() - t0)
             t = plan.timings()
             launches += plan.gram_timing()["launches"]
+            placed += plan.placement()["placed_last"]
             dev_ms.append(t["total"])
             integ_ms.append(t["integrate"])
             subs = 10 * (T_MS + 1) + 100_000 * np.asarray(r["fic_ntrials"], np.float64)[a:b] if dist else \
@@ -385,7 +400,8 @@ def run_b200(args):
             "config": workload_config(world),
             "impl_config": {"precision": "f32 integration, f64 FIC/centring", "gram": args.gram,
                             "integrator": plan.integrator(), "window_tile": plan.window_tile(),
-                            "noise": "philox table", "graph_launched": plan.graph_launched()},
+                            "noise": "philox table", "graph_launched": plan.graph_launched(),
+                            "placement": {**plan.placement(), "placed_steps": placed}},
             "e2e": {"value": e2e, "unit": "sims/s", "h2d_bytes_per_step": 8 * (n + 2 * n * N),
                     "d2h_bytes_per_step": 8 * n * 5 + 4 * n * 3 + 8 * n * N},
             "gpu_launches": launches,

@@ -98,6 +98,7 @@ def lib():
         L.bnm_bw_math_probe.argtypes = [i32, vp, i32, vp]
         L.bnm_wait_probe.argtypes = [i32, C.c_int64, vp, vp]
         L.bnm_plan_graph.argtypes = [vp, vp]
+        L.bnm_plan_placement.argtypes = [vp, vp, vp]
         L.bnm_plan_window_tile.argtypes = [vp, vp, vp]
         L.bnm_philox_probe.argtypes = [i32, vp, i32, vp]
         L.bnm_calculate_params.argtypes = [i32, i32, i32, vp, dbl, dbl, dbl, dbl, vp, vp, vp, vp, vp]
@@ -288,6 +289,12 @@ class Plan:
         g = C.c_int32()
         _check(lib().bnm_plan_graph(self._h, C.byref(g)))
         return bool(g.value)
+
+    def placement(self) -> dict:
+        """Particle placement state (bnm_plan_placement)."""
+        e, l = C.c_int32(), C.c_int32()
+        _check(lib().bnm_plan_placement(self._h, C.byref(e), C.byref(l)))
+        return dict(enabled=bool(e.value), placed_last=bool(l.value))
 
     def integrator(self) -> dict:
         """FP32 integrator shape the autotuner picked for the last batch size."""

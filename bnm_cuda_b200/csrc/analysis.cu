@@ -16,7 +16,8 @@
 //     co-moments of the globally centred series, updated by one add and one
 //     subtract per frame as the window slides, so window FC costs O(P) per
 //     window instead of O(P*L).  Static FC comes from the same pass.  Window
-//     sums over pairs (for the FCD centring) are reduced in FP64.
+//     sums over pairs (for the FCD centring) follow in window_sums_kernel,
+//     FP64 in a fixed order, so the FCD does not depend on the window tile.
 //   * fcd_gram_kernel: FCD = Z Z^T over the centred, unit-norm window-FC rows
 //     (64x64 output tiles, FP32), lower triangle only; its epilogue drops each
 //     FCD value into the KS histogram (upper_bound rank among the sorted
@@ -45,8 +46,7 @@ __global__ void __launch_bounds__(256) fc_window_kernel(FcArgs a, const TB* __re
     double* fss = fs + N;
     double* ws = fss + N;                                 // current-window sums [N]
     double* wss = ws + N;
-    double* red = wss + N;                                // [2]
-    TB* ring = reinterpret_cast<TB*>(red + 2);            // last L frames [L][N]
+    TB* ring = reinterpret_cast<TB*>(wss + N);            // last L frames [L][N]
 
     const int sim = blockIdx.x;
     const int p0 = blockIdx.y * (blockDim.x * PPT);
@@ -99,7 +99,6 @@ __global__ void __launch_bounds__(256) fc_window_kernel(FcArgs a, const TB* __re
         }
         if (k < a.W && t == k * a.win_step + L - 1) {
             __syncthreads();  // node window sums complete
-            double s1 = 0.0, s2 = 0.0;
             const double invL = 1.0 / L;
 #pragma unroll
             for (int u = 0; u < PPT; u++) {
@@ -112,22 +111,8 @@ __global__ void __launch_bounds__(256) fc_window_kernel(FcArgs a, const TB* __re
                 const float rf = (float)r;
                 if (!(r == r) || isinf(r)) any_nan = true;
                 a.wfc[((size_t)sim * a.W + k) * a.P + p0 + u * blockDim.x + threadIdx.x] = rf;
-                s1 += rf;
-                s2 += (double)rf * rf;
             }
-            s1 = warp_sum(s1);
-            s2 = warp_sum(s2);
-            if (threadIdx.x == 0) red[0] = red[1] = 0.0;
-            __syncthreads();
-            if ((threadIdx.x & 31) == 0) {
-                atomicAdd(&red[0], s1);
-                atomicAdd(&red[1], s2);
-            }
-            __syncthreads();
-            if (threadIdx.x == 0) {
-                atomicAdd(&a.wsum[((size_t)sim * a.W + k) * 2 + 0], red[0]);
-                atomicAdd(&a.wsum[((size_t)sim * a.W + k) * 2 + 1], red[1]);
-            }
+            __syncthreads();  // every pair has read this window's node sums
             // slide to window k+1: drop the frames it no longer covers
             const int nlo = (k + 1) * a.win_step;
             if (nlo <= t) {
@@ -365,7 +350,7 @@ template <typename TB, int PPT>
 static cudaError_t launch_fc_window_t(const FcArgs& a, const TB* bold, cudaStream_t st) {
     constexpr int TPB = 256;
     const int chunks = (a.P + TPB * PPT - 1) / (TPB * PPT);
-    const size_t smem = (size_t)a.N * 5 * sizeof(double) + 2 * sizeof(double) + (size_t)a.win_len * a.N * sizeof(TB);
+    const size_t smem = (size_t)a.N * 5 * sizeof(double) + (size_t)a.win_len * a.N * sizeof(TB);
     if (smem > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(fc_window_kernel<TB, PPT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -389,7 +374,11 @@ static cudaError_t launch_fc_window(const FcArgs& a, const TB* bold, cudaStream_
 }
 
 cudaError_t bnm_launch_fc_window(const FcArgs& a, cudaStream_t st) {
-    return a.bold_f64 ? launch_fc_window<double>(a, a.bold_f64, st) : launch_fc_window<float>(a, a.bold, st);
+    cudaError_t e = a.bold_f64 ? launch_fc_window<double>(a, a.bold_f64, st) : launch_fc_window<float>(a, a.bold, st);
+    if (e != cudaSuccess || a.W < 1) return e;
+    // The window rows' sums over all pairs, in a fixed order: the same BOLD
+    // gives the same FCD whatever the window tile and the launch order.
+    return bnm_launch_window_sums(a.wfc, a.n_sims, a.W, a.P, 0, a.P, a.wsum, st);
 }
 
 // Window-FC sums over a pair range, one CTA per (window, simulation): the

@@ -62,7 +62,8 @@ struct SimArgs {
     int* failed;        // [n]
     double* ext;        // [n][6][N] means of S_E, I_E, r_E, S_I, I_I, r_I over kept frames
     int* work_counter;  // persistent scheduling (zeroed before launch)
-    const int* order;   // optional placement: CTA b's first particle is order[b], later claims order[grid + k]
+    const int* order;   // optional placement: particles by predicted work, heaviest first
+    int* place_ws;      // with order: [0, 2) a 64-bit two-ended claim word, [2, 2 + 256) CTAs per SM (zeroed)
     int* status;
 };
 

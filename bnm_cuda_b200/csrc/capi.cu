@@ -129,6 +129,8 @@ extern "C" int bnm_config_sizes(const bnm_config* c, bnm_sizes* s) {
     return BNM_OK;
 }
 
+constexpr int kPlaceWs = 2 + 256;  // placement claim word + CTAs per SM
+
 struct bnm_plan {
     bnm_config cfg;
     bnm_sizes sz;
@@ -177,10 +179,13 @@ struct bnm_plan {
     int run_graph_n = 0, last_graph = 0;
     // window-FC tile (pairs per thread) picked by the tuner for batches of win_tuned_n particles
     int win_ppt = 0, win_tuned_n = 0, win_tried = 0;
-    // placement of particles on the register kernel's CTAs by predicted FIC work (BNM_B200_PLACE=1):
-    // the parameters and FIC restart counts of the particles simulated so far
+    // placement of particles on the register kernel's CTAs by predicted FIC work (on by
+    // default; BNM_B200_PLACE=0 turns it off): the predicted order, the claim counters,
+    // and the parameters and FIC restart counts of the particles simulated so far
     bool place = false;
+    bool last_placed = false;  // the last run's order came from the history
     int* d_order = nullptr;
+    int* d_place_ws = nullptr;  // kPlaceWs ints, zeroed before each launch
     int* io_order = nullptr;  // pinned [max_sims]
     std::vector<float> hist_x;  // G, mean wEE, mean wEI per simulated particle
     std::vector<int> hist_tr;
@@ -306,11 +311,14 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
                                            p->num_sms, p->st));
     }
 
-    // particle placement (register kernel, numerical FIC; opt-in)
-    if (const char* pl = std::getenv("BNM_B200_PLACE"))
-        p->place = !std::strcmp(pl, "1") && cfg->precision == BNM_PREC_F32 && p->kmax && cfg->do_fic &&
-                   cfg->numerical_fic;
+    // particle placement (register kernel with a noise table, numerical FIC; BNM_B200_PLACE=0 turns it off)
+    {
+        const char* pl = std::getenv("BNM_B200_PLACE");
+        p->place = !(pl && !std::strcmp(pl, "0")) && cfg->precision == BNM_PREC_F32 && p->kmax && cfg->do_fic &&
+                   cfg->numerical_fic && p->d_noise;
+    }
     if (p->place) {
+        BNM_CUDA_TRY(dalloc(p, &p->d_place_ws, kPlaceWs));
         BNM_CUDA_TRY(dalloc(p, &p->d_order, (size_t)cfg->max_sims));
         BNM_CUDA_TRY(cudaMallocHost((void**)&p->io_order, (size_t)cfg->max_sims * sizeof(int)));
         for (int i = 0; i < cfg->max_sims; i++) p->io_order[i] = i;
@@ -528,6 +536,7 @@ static int tune_integrator(bnm_plan* p, const SimArgs& a, bool share = false) {
     SimArgs t = a;
     t.T = std::min(a.T, 200);
     t.adjust_fic = 0;
+    t.order = nullptr;  // shapes are timed on claim order
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_status, 0, 16, p->st));
     double best = 1e300;
     for (int i = 0; i < nc; i++) {
@@ -645,8 +654,7 @@ static int launch_window_only(bnm_plan* p, int n) {
 // Window-tile tuner: times the window-FC kernel with 1, 2, 4 and 8 pairs per
 // thread (256, 512, 1024 and 2048 pairs per CTA) on this batch size and keeps
 // the fastest, on the first run of each batch size (BNM_B200_TUNE=0: 4).  The
-// timing launches accumulate into the window sums and NaN flags, which are
-// cleared afterwards.
+// timing launches accumulate into the NaN flags, which are cleared afterwards.
 static int tune_window(bnm_plan* p, int n) {
     if (p->win_tuned_n == n) return BNM_OK;
     const char* tune = std::getenv("BNM_B200_TUNE");
@@ -691,7 +699,7 @@ static int launch_analysis(bnm_plan* p, int n, int calc_fic_penalty, bool hemis)
     const int N = c.nodes;
     cudaStream_t st = p->st;
     p->n_gram = 0;
-    p->launches += 2;  // window FC and goodness of fit
+    p->launches += c.no_fcd ? 2 : 3;  // window FC (+ window sums) and goodness of fit
 
     BNM_CUDA_TRY(bnm_launch_fc_window(fc_args(p, n), st));
     const int split = c.gram == BNM_GRAM_BF16_SPLIT;
@@ -924,6 +932,7 @@ static SimArgs sim_args(bnm_plan* p, int n) {
     a.wEI = p->d_wEI;
     a.wIE = p->d_wIE;
     a.order = p->place ? p->d_order : nullptr;
+    a.place_ws = p->d_place_ws;
     a.noise = p->d_noise;  // NULL: the register integrator draws Philox noise in place
     a.noise_seed = c.noise_seed;
     a.noise_ld = p->noise_ld;
@@ -946,22 +955,25 @@ static int ensure_pinned(bnm_plan* p);
 static int enqueue_run(bnm_plan* p, int n);
 static int read_timings(bnm_plan* p);
 
-// Particle placement on the register kernel's CTAs (BNM_B200_PLACE=1).  A
+// Particle placement on the register kernel's CTAs (on by default for that
+// kernel with a noise table and numerical FIC; BNM_B200_PLACE=0 turns it off).  A
 // particle that hits the numerical-FIC trial cap integrates about 1 M more
 // substeps than one that needs no restart, and with more particles than SMs
 // the CTAs share SMs (two per SM, each slower than alone), so the generation
-// ends with the heavy particles that shared an SM.  CTA b starts with the
-// particle at position b of io_order; the first num_sms CTAs go to distinct
-// SMs and CTA num_sms + k joins CTA k's SM, so positions [n - S, S) run alone.
-// Work is predicted by the FIC restart count of the nearest particle simulated
-// before by this plan (G, mean wEE, mean wEI, each scaled by its spread); the
-// heaviest take the lone positions, the others pair heaviest with lightest.
-// Without history the order is the identity.
+// ends with the heavy particles that shared an SM.  The kernel hands out
+// io_order from both ends: the second CTA on an SM takes the lightest
+// particles, every other CTA the heaviest, so heavy particles run alone or
+// beside light ones.  Work is predicted by the FIC restart count of the
+// nearest particle simulated before by this plan (G, mean wEE, mean wEI, each
+// scaled by its spread); io_order lists the particles heaviest first.
+// Without history (fewer than 16 particles) the order is the identity.  Where
+// a particle runs does not change its results.
 static void place_particles(bnm_plan* p, int n, const double* G, const double* w_ee, const double* w_ei) {
-    const int N = p->cfg.nodes, S = p->num_sms;
+    const int N = p->cfg.nodes;
     for (int i = 0; i < n; i++) p->io_order[i] = i;
     const size_t H = p->hist_tr.size();
-    if (H < 16 || n <= 1) return;
+    p->last_placed = H >= 16 && n > 1;
+    if (!p->last_placed) return;
     double mu[3] = {0, 0, 0}, sd[3] = {0, 0, 0};
     for (size_t h = 0; h < H; h++)
         for (int d = 0; d < 3; d++) mu[d] += p->hist_x[3 * h + d];
@@ -991,27 +1003,14 @@ static void place_particles(bnm_plan* p, int n, const double* G, const double* w
             }
         }
     }
-    std::vector<int> by(n);
-    for (int i = 0; i < n; i++) by[i] = i;
-    std::stable_sort(by.begin(), by.end(), [&](int a, int b) { return pred[a] > pred[b]; });
-    if (n <= S || n > 2 * S) {  // every CTA alone, or more particles than CTAs: heaviest first
-        for (int i = 0; i < n; i++) p->io_order[i] = by[i];
-        return;
-    }
-    const int pairs = n - S, lone = S - pairs;
-    for (int k = 0; k < lone; k++) p->io_order[pairs + k] = by[k];
-    const int* rest = by.data() + lone;  // 2 * pairs particles, heaviest first
-    for (int k = 0; k < pairs; k++) {
-        p->io_order[k] = rest[k];
-        p->io_order[S + k] = rest[2 * pairs - 1 - k];
-    }
+    std::stable_sort(p->io_order, p->io_order + n, [&](int a, int b) { return pred[a] > pred[b]; });
 }
 
 // Appends the last batch's particles and FIC restart counts to the placement history.
 static void record_particles(bnm_plan* p, int n, const double* G, const double* w_ee, const double* w_ei,
                              const int* trials) {
     const int N = p->cfg.nodes;
-    const size_t cap = 1 << 14;
+    const size_t cap = 4096;  // the most recent particles (a few generations)
     for (int i = 0; i < n; i++) {
         float x[3] = {(float)G[i], 0.f, 0.f};
         double e = 0, f = 0;
@@ -1156,6 +1155,7 @@ extern "C" int bnm_run(bnm_plan* p, int32_t n, const double* G, const double* w_
             BNM_CUDA_TRY(cudaStreamSynchronize(st));  // the tuner's launches may still read the order
             place_particles(p, n, G, w_ee, w_ei);
             BNM_CUDA_TRY(cudaMemcpyAsync(p->d_order, p->io_order, n * 4, cudaMemcpyHostToDevice, st));
+            BNM_CUDA_TRY(cudaMemsetAsync(p->d_place_ws, 0, kPlaceWs * 4, st));
         }
         BNM_CUDA_TRY(bnm_launch_integrate_shape(a, p->shape, p->num_sms, st));
     }
@@ -1271,7 +1271,10 @@ static int enqueue_run(bnm_plan* p, int n) {
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_hist, 0, (size_t)n * (p->m + 1) * 4, st));
     BNM_CUDA_TRY(cudaMemsetAsync(p->d_eq, 0, (size_t)n * (p->m + 1) * 4, st));
     const SimArgs a = sim_args(p, n);
-    if (p->place) BNM_CUDA_TRY(cudaMemcpyAsync(p->d_order, p->io_order, n * 4, cudaMemcpyHostToDevice, st));
+    if (p->place) {
+        BNM_CUDA_TRY(cudaMemcpyAsync(p->d_order, p->io_order, n * 4, cudaMemcpyHostToDevice, st));
+        BNM_CUDA_TRY(cudaMemsetAsync(p->d_place_ws, 0, kPlaceWs * 4, st));
+    }
     if (c.precision == BNM_PREC_F32)
         BNM_CUDA_TRY(bnm_launch_integrate_shape(a, p->shape, p->num_sms, st));
     else
@@ -1535,6 +1538,13 @@ extern "C" int bnm_plan_window_tile(bnm_plan* p, int32_t* pairs_per_thread, int3
 extern "C" int bnm_plan_graph(bnm_plan* p, int32_t* graph_launched) {
     if (!p || !graph_launched) return fail(BNM_EINVAL, "null argument");
     *graph_launched = p->last_graph;
+    return BNM_OK;
+}
+
+extern "C" int bnm_plan_placement(bnm_plan* p, int32_t* enabled, int32_t* placed_last) {
+    if (!p || !enabled || !placed_last) return fail(BNM_EINVAL, "null argument");
+    *enabled = p->place;
+    *placed_last = p->place && p->last_placed;
     return BNM_OK;
 }
 

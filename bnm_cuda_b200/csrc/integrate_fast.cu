@@ -70,9 +70,10 @@ struct Slot {
 // and substep pair gives the E and I values of both substeps) instead of
 // being streamed from the table through the TMA ring; the values are the
 // table's, so both give the same results.
-template <int K, int KC, int P, bool NZI>
+template <int K, int KC, int P, bool NZI, bool PL = false>
 __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
     static_assert(K % 4 == 0 && K <= 32, "K");
+    static_assert(!PL || (P == 1 && !NZI), "placement: one particle per CTA, table noise");
     static_assert(KC % 2 == 0 && KC <= K && KC + 2 >= K, "KC");
     static_assert(P >= 1 && P <= 2, "P");
     constexpr int LD = 4 * K;  // padded SC row length and S_E buffer length (quarter v at K v)
@@ -166,15 +167,33 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
         }
     };
     // take the next particle of the batch into slot p (all threads)
-    // With a placement order (one particle per CTA only) CTA b starts with the
-    // particle the host put at position b and later claims continue after the
-    // grid; without one, particles go out in claim order.
-    const bool placed = P == 1 && a.order != nullptr;
-    auto load = [&](int p, bool initial) {
+    // PL (placement, one particle per CTA, table noise): a.order lists the
+    // particles by predicted work, heaviest first.  A CTA that arrives second
+    // on its SM takes particles from the light end, every other CTA from the
+    // heavy end, so a heavy particle runs alone on an SM or beside a light
+    // one, wherever the hardware put the CTAs.  One 64-bit counter holds the
+    // heavy claims (high half) and the light claims (low half); a claim is
+    // valid while the claims before it number fewer than the particles.  A
+    // separate instantiation: claim code in the default kernel changed the
+    // code generated for its substep loop and cost 14 %.
+    __shared__ int s_light;
+    if constexpr (PL) {
         if (threadIdx.x == 0) {
-            const int c = placed && initial ? (int)blockIdx.x
-                                            : atomicAdd(a.work_counter, 1) + (placed ? (int)gridDim.x : 0);
-            s_sim[p] = c < a.n_sims ? (placed ? a.order[c] : c) : a.n_sims;
+            unsigned smid;
+            asm volatile("mov.u32 %0, %%smid;" : "=r"(smid));
+            s_light = smid < 256 && atomicAdd(a.place_ws + 2 + smid, 1) >= 1;
+        }
+    }
+    auto load = [&](int p) {
+        if (threadIdx.x == 0) {
+            if constexpr (PL) {
+                const unsigned long long c = atomicAdd(reinterpret_cast<unsigned long long*>(a.place_ws),
+                                                       s_light ? 1ull : 1ull << 32);
+                const int heavy = (int)(c >> 32), light = (int)(unsigned)c;
+                s_sim[p] = heavy + light < a.n_sims ? a.order[s_light ? a.n_sims - 1 - light : heavy] : a.n_sims;
+            } else {
+                s_sim[p] = atomicAdd(a.work_counter, 1);
+            }
         }
         __syncthreads();
         sim[p] = s_sim[p];
@@ -210,7 +229,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
 #pragma unroll
     for (int p = 0; p < P; p++) {
         c_cons[p] = c_issue[p] = 0;
-        load(p, true);
+        load(p);
     }
     int cur = 0;
 
@@ -460,7 +479,7 @@ __global__ void __launch_bounds__(128, 1) integrate_fast_kernel(SimArgs a) {
                     a.trials[sim[p]] = trial[p];
                     a.failed[sim[p]] = failed[p] ? 1 : 0;
                 }
-                load(p, false);
+                load(p);
             }
         }
         if (timed_out) break;
@@ -496,6 +515,15 @@ static cudaError_t launch_fast(const SimArgs& a, int grid, cudaStream_t st) {
         return cudaGetLastError();
     }
     const size_t smem = fast_smem<K, KC, P, false>(a.N, threads);
+    if constexpr (P == 1) {
+        if (a.order) {  // placement
+            cudaError_t e = cudaFuncSetAttribute(integrate_fast_kernel<K, KC, 1, false, true>,
+                                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            if (e != cudaSuccess) return e;
+            integrate_fast_kernel<K, KC, 1, false, true><<<grid, threads, smem, st>>>(a);
+            return cudaGetLastError();
+        }
+    }
     cudaError_t e = cudaFuncSetAttribute(integrate_fast_kernel<K, KC, P, false>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;

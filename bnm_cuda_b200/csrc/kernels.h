@@ -17,7 +17,7 @@ struct FcArgs {
     const double* bold_f64;   // [n][frames][N] (FP64 integrator); exactly one is set
     float* fc;                // [n][P]
     float* wfc;               // [n][W][P] raw window FC
-    double* wsum;             // [n][W][2] sum, sum of squares over pairs (zeroed)
+    double* wsum;             // [n][W][2] sum, sum of squares over pairs (written after the window FC)
     int* nan_flag;            // [n]
     int ppt;                  // pairs per thread: a CTA of 256 threads covers 256 ppt pairs (0: 4)
 };

@@ -19,6 +19,8 @@ two-sample KS of the device's own FCD values (to the last bits of the final
 division), and lie within 1e-2
 (BF16) / 2e-3 (F32, split) of the KS of the FP64 FCD.
 """
+import concurrent.futures as cf
+
 import numpy as np
 import pytest
 
@@ -38,8 +40,14 @@ TOL = {B.GRAM_F32: (1e-6, 2e-5, 2e-3), B.GRAM_BF16: (2e-3, 1e-3, 1e-2), B.GRAM_B
 NAMES = {B.GRAM_F32: "f32", B.GRAM_BF16: "bf16", B.GRAM_BF16_SPLIT: "bf16x3"}
 
 
+# The precision-stress shape (N = 400, all 79,800 pairs, TR 0.5 s, window 44
+# step 1) on 200 s of model time with 10 s removed: 381 frames, 337 windows,
+# 56,616 FCD entries, 3 FCD row blocks, 1247 K tiles (cluster integrator).
+CONFIG2_SHAPE = (400, 200000, 500, 44, 1, 10, False)
+
+
 def _run_all(case, n=3):
-    N, T, TR, ws, step, remove, exc = CASES[case]
+    N, T, TR, ws, step, remove, exc = CASES[case] if isinstance(case, str) else case
     sc = synth.make_sc(N, 0.3, 5)
     G, wEE, wEI = synth.uniform_params(n, N, seed=11)
     rng = np.random.default_rng(3)
@@ -54,19 +62,22 @@ def _run_all(case, n=3):
     return cfg, emp_fcd, res
 
 
-@pytest.mark.parametrize("case", list(CASES))
-def test_tensor_core_grams_against_fp64_oracle(case, port):
-    cfg, emp_fcd, res = _run_all(case)
-    N, T, TR, ws, step, remove, exc = CASES[case]
+def _grams_against_oracle(case, port, n=3):
+    cfg, emp_fcd, res = _run_all(case, n)
+    N, T, TR, ws, step, remove, exc = CASES[case] if isinstance(case, str) else case
     nvr = cfg.sizes()["n_vols_remove"]
     bold = res[B.GRAM_F32]["bold"]
     errs = {}
     for gram, r in res.items():
         np.testing.assert_array_equal(r["bold"], bold)
-    for i in range(len(bold)):
+
+    def oracle(i):
         kept = bold[i][nvr:]
-        fc64 = port.port_fc_tril(kept, exc=exc)
-        fcd64 = port.port_fcd_tril(kept, step, ws, exc=exc)
+        return port.port_fc_tril(kept, exc=exc), port.port_fcd_tril(kept, step, ws, exc=exc)
+
+    with cf.ThreadPoolExecutor(len(bold)) as ex:  # the port releases the GIL
+        ref = list(ex.map(oracle, range(len(bold))))
+    for i, (fc64, fcd64) in enumerate(ref):
         ks64 = port.port_ks(emp_fcd, fcd64)
         for gram, r in res.items():
             e = (np.abs(r["fc"][i] - fc64).max(), np.abs(r["fcd"][i] - fcd64).max(), abs(r["fcd_ks"][i] - ks64))
@@ -75,6 +86,21 @@ def test_tensor_core_grams_against_fp64_oracle(case, port):
     print(case, {k: [f"{x:.2e}" for x in v] for k, v in errs.items()})
     for gram in res:
         assert np.all(errs[NAMES[gram]] <= np.array(TOL[gram])), (NAMES[gram], errs[NAMES[gram]])
+    return cfg
+
+
+@pytest.mark.parametrize("case", list(CASES))
+def test_tensor_core_grams_against_fp64_oracle(case, port):
+    _grams_against_oracle(case, port)
+
+
+def test_config2_shape_grams_against_fp64_oracle(port):
+    """Every Gram arithmetic at the precision-stress workload's node count,
+    pair count, TR and window (CONFIG2_SHAPE) against the FP64 oracle
+    (check_fit.cpp:19-134 restated) on the same BOLD, two particles."""
+    cfg = _grams_against_oracle(CONFIG2_SHAPE, port, n=2)
+    s = cfg.sizes()
+    assert (s["n_pairs"], s["frames"] - s["n_vols_remove"], s["n_windows"]) == (79800, 381, 337)
 
 
 def test_staged_chunks_give_the_same_result(monkeypatch):

@@ -130,11 +130,13 @@ def test_single_plan_generation_is_one_graph_launch(N, monkeypatch):
 
 
 def test_particle_placement_keeps_every_particles_result(monkeypatch):
-    """BNM_B200_PLACE=1: the register kernel's CTAs take particles in an order
-    predicted from the plan's history (heaviest FIC work on the CTAs that are
-    alone on an SM).  Placement changes only where a particle runs, so every
-    particle's results must equal those of the unplaced plan, bit for bit,
-    with more particles than SMs (paired and lone CTAs) and on the graph path."""
+    """Particle placement (on by default for the register kernel): the CTAs
+    take particles in an order predicted from the plan's history (heaviest
+    FIC work on the CTAs alone on an SM, the lightest on the second CTA of an
+    SM).  Placement changes only where a particle runs, so every particle's
+    results must equal those of the unplaced plan (BNM_B200_PLACE=0), bit for
+    bit, with more particles than SMs (paired and lone CTAs) and on the graph
+    path."""
     N, n = 20, 200
     sc = synth.make_sc(N, 0.3, 6)
     cfg = B.Config(nodes=N, max_sims=n, time_steps=12000, bold_tr=500, window_size=10, window_step=2,
@@ -144,17 +146,20 @@ def test_particle_placement_keeps_every_particles_result(monkeypatch):
     emp_fc, emp_fcd = rng.uniform(-0.2, 0.8, s["n_pairs"]), rng.uniform(-0.3, 1.0, 300)
     P1, P2 = synth.uniform_params(n, N, 50), synth.uniform_params(n, N, 51)
     monkeypatch.setenv("BNM_B200_SLOTS", "1")
+    monkeypatch.setenv("BNM_B200_PLACE", "0")
     with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+        assert p.placement() == dict(enabled=False, placed_last=False)
         ref = [p.run(*P1), p.run(*P2)]
-    monkeypatch.setenv("BNM_B200_PLACE", "1")
+    monkeypatch.delenv("BNM_B200_PLACE")
     with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
         got = [p.run(*P1)]  # no history yet: identity order
+        assert p.placement() == dict(enabled=True, placed_last=False)
         monkeypatch.setenv("BNM_B200_GRAPH", "0")
         got.append(p.run(*P2))  # placed, eager
-        assert not p.graph_launched()
+        assert not p.graph_launched() and p.placement()["placed_last"]
         monkeypatch.delenv("BNM_B200_GRAPH")
         got.append(p.run(*P2))  # placed, graph launch
-        assert p.graph_launched()
+        assert p.graph_launched() and p.placement()["placed_last"]
     for a, b in ((ref[0], got[0]), (ref[1], got[1]), (ref[1], got[2])):
         _same(a, b)
         np.testing.assert_array_equal(a["cost"], b["cost"])
