@@ -1447,6 +1447,8 @@ extern "C" int bnm_group_run(bnm_group* g, const int32_t* n, const double* const
             p->io_wEI[k] = rf ? (double)(float)w_ei[i][k] : w_ei[i][k];
         }
         sizes[i] = n[i];
+        // the captured graph copies io_order at launch, so it is set for every run
+        if (p->place) place_particles(p, n[i], p->io_G, p->io_wEE, p->io_wEI);
     }
     int rc;
     if (!g->exec || sizes != g->n) {
@@ -1509,6 +1511,7 @@ extern "C" int bnm_group_run(bnm_group* g, const int32_t* n, const double* const
         put(o.fic_failed, p->io_failed, k);
         put(o.fic_ntrials, p->io_trials, k);
         put(o.fic_unstable, p->io_unstable, k);
+        if (p->place) record_particles(p, k, p->io_G, p->io_wEE, p->io_wEI, p->io_trials);
     }
     return BNM_OK;
 }

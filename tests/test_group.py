@@ -163,3 +163,32 @@ def test_particle_placement_keeps_every_particles_result(monkeypatch):
     for a, b in ((ref[0], got[0]), (ref[1], got[1]), (ref[1], got[2])):
         _same(a, b)
         np.testing.assert_array_equal(a["cost"], b["cost"])
+
+
+def test_group_places_its_own_batch_after_a_larger_run(monkeypatch):
+    """A plan whose last bnm_run placed a larger batch (an order over 40
+    particles) then runs 12 particles in a group, eagerly and as a graph: the
+    group sets the order for its own batch, so every particle is simulated
+    and the results equal an unplaced plan's."""
+    N = 20
+    sc = synth.make_sc(N, 0.3, 6)
+    cfg = B.Config(nodes=N, max_sims=40, time_steps=12000, bold_tr=500, window_size=10, window_step=2,
+                   bold_remove_s=2)
+    s = cfg.sizes()
+    rng = np.random.default_rng(3)
+    emp_fc, emp_fcd = rng.uniform(-0.2, 0.8, s["n_pairs"]), rng.uniform(-0.3, 1.0, 300)
+    big, small = synth.uniform_params(40, N, 60), synth.uniform_params(12, N, 61)
+    monkeypatch.setenv("BNM_B200_SLOTS", "1")
+    monkeypatch.setenv("BNM_B200_PLACE", "0")
+    with B.Plan(cfg, sc, emp_fc, emp_fcd) as q:
+        want = q.run(*small, outputs=("w_ie",))
+    monkeypatch.delenv("BNM_B200_PLACE")
+    p = B.Plan(cfg, sc, emp_fc, emp_fcd)
+    p.run(*big)
+    p.run(*big)
+    assert p.placement()["placed_last"]
+    with B.Group([p]) as g:
+        for _ in range(2):  # eager (tunes for 12), then the graph
+            _same(want, g.run([small])[0])
+        assert g.last()["graph"]
+    p.close()
