@@ -311,11 +311,12 @@ static int plan_create(const bnm_config* cfg, const double* sc, const double* em
                                            p->num_sms, p->st));
     }
 
-    // particle placement (register kernel with a noise table, numerical FIC; BNM_B200_PLACE=0 turns it off)
+    // particle placement (numerical FIC, FP32: the register kernel with a noise table, the
+    // column-split clusters; BNM_B200_PLACE=0 turns it off)
     {
         const char* pl = std::getenv("BNM_B200_PLACE");
-        p->place = !(pl && !std::strcmp(pl, "0")) && cfg->precision == BNM_PREC_F32 && p->kmax && cfg->do_fic &&
-                   cfg->numerical_fic && p->d_noise;
+        p->place = !(pl && !std::strcmp(pl, "0")) && cfg->precision == BNM_PREC_F32 && cfg->do_fic &&
+                   cfg->numerical_fic && (p->kmax ? p->d_noise != nullptr : true);
     }
     if (p->place) {
         BNM_CUDA_TRY(dalloc(p, &p->d_place_ws, kPlaceWs));
@@ -955,8 +956,11 @@ static int ensure_pinned(bnm_plan* p);
 static int enqueue_run(bnm_plan* p, int n);
 static int read_timings(bnm_plan* p);
 
-// Particle placement on the register kernel's CTAs (on by default for that
-// kernel with a noise table and numerical FIC; BNM_B200_PLACE=0 turns it off).  A
+// Particle placement (on by default with numerical FIC on the FP32 path: the
+// register kernel with a noise table, the column-split clusters;
+// BNM_B200_PLACE=0 turns it off).  Column-split clusters of two particles
+// integrate io_order's pairs, so the two particles they advance in lockstep
+// need about the same number of substeps.  In the register kernel a
 // particle that hits the numerical-FIC trial cap integrates about 1 M more
 // substeps than one that needs no restart, and with more particles than SMs
 // the CTAs share SMs (two per SM, each slower than alone), so the generation

@@ -107,7 +107,10 @@ __global__ void integrate_colsplit_kernel(SimArgs a, int R) {
     const int tu = P == 1 ? t : t - slot * HB;  // own node index of this thread
     const int sim_raw = (int)(blockIdx.x / csize) * P + slot;
     const bool live = P == 1 || sim_raw < a.n_sims;
-    const int sim = live ? sim_raw : sim_raw - slot;
+    // with a placement order, cluster c integrates particles order[P c ..]: the
+    // order lists them by predicted work, so the particles a cluster advances
+    // in lockstep need about the same number of substeps
+    const int sim = a.order ? a.order[live ? sim_raw : sim_raw - slot] : (live ? sim_raw : sim_raw - slot);
     const int r0 = (int)crank * R;
     const int r_own = max(0, min(N - r0, R));  // nodes this CTA updates
     const int upd_warps = (r_own + 31) >> 5;    // warps (per particle) holding node owners

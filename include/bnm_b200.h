@@ -162,12 +162,13 @@ int bnm_run(bnm_plan *plan, int32_t n, const double *G, const double *w_ee, cons
 /* Whether the plan's last bnm_run was a graph launch (1) or eager (0). */
 int bnm_plan_graph(bnm_plan *plan, int32_t *graph_launched);
 
-/* Particle placement of the register integrator (N <= 128, FP32, noise table,
- * numerical FIC; no counterpart in the reference, whose blocks take particles
- * by index): the plan predicts each particle's FIC restarts from the nearest
- * of the last 4096 particles it simulated, and the kernel gives the heaviest
- * particles to CTAs alone on an SM and the lightest to the second CTA of an
- * SM.  Results do not depend on it.  enabled: the plan places particles
+/* Particle placement (FP32, numerical FIC; no counterpart in the reference,
+ * whose blocks take particles by index): the plan predicts each particle's FIC
+ * restarts from the nearest of the last 4096 particles it simulated.  The
+ * register integrator (N <= 128, noise table) gives the heaviest particles to
+ * CTAs alone on an SM and the lightest to the second CTA of an SM; the
+ * two-particle column-split clusters pair particles of similar predicted work.
+ * Results do not depend on it.  enabled: the plan places particles
  * (BNM_B200_PLACE=0 at plan creation turns it off); placed_last: the last
  * run's order came from the history (16 particles or more simulated before). */
 int bnm_plan_placement(bnm_plan *plan, int32_t *enabled, int32_t *placed_last);

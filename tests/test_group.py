@@ -192,3 +192,38 @@ def test_group_places_its_own_batch_after_a_larger_run(monkeypatch):
             _same(want, g.run([small])[0])
         assert g.last()["graph"]
     p.close()
+
+
+def test_cluster_pairing_by_predicted_work_keeps_every_particles_result(monkeypatch):
+    """Two-particle column-split clusters (N = 200) with placement: after the
+    first batch a cluster advances two particles of similar predicted FIC
+    work instead of two neighbours by index.  A particle's results do not
+    depend on its partner (a restart the partner asks for reruns it bit for
+    bit), so they must equal the unplaced plan's, eagerly and as a graph."""
+    N, n = 200, 16  # one batch of 16 is the history placement needs
+    sc = synth.make_sc(N, 0.3, 7)
+    cfg = B.Config(nodes=N, max_sims=n, time_steps=12000, bold_tr=500, window_size=10, window_step=2,
+                   bold_remove_s=2)
+    s = cfg.sizes()
+    rng = np.random.default_rng(4)
+    emp_fc, emp_fcd = rng.uniform(-0.2, 0.8, s["n_pairs"]), rng.uniform(-0.3, 1.0, 300)
+    P1, P2 = synth.uniform_params(n, N, 70), synth.uniform_params(n, N, 71)
+    monkeypatch.setenv("BNM_B200_SHAPE", "4,25,4,2,25")
+    monkeypatch.setenv("BNM_B200_PLACE", "0")
+    with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+        ref = p.run(*P2, outputs=("bold", "w_ie"))
+    monkeypatch.delenv("BNM_B200_PLACE")
+    with B.Plan(cfg, sc, emp_fc, emp_fcd) as p:
+        p.run(*P1)
+        assert p.placement() == dict(enabled=True, placed_last=False)
+        monkeypatch.setenv("BNM_B200_GRAPH", "0")
+        got = [p.run(*P2, outputs=("bold", "w_ie"))]  # placed, eager
+        assert p.placement()["placed_last"] and not p.graph_launched()
+        monkeypatch.delenv("BNM_B200_GRAPH")
+        got.append(p.run(*P2, outputs=("bold", "w_ie")))  # placed, graph launch
+        assert p.graph_launched()
+        assert p.integrator()["kind"] == "colsplit2"
+    for g in got:
+        _same(ref, g)
+        np.testing.assert_array_equal(ref["cost"], g["cost"])
+        np.testing.assert_array_equal(ref["bold"], g["bold"])
