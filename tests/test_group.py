@@ -129,15 +129,17 @@ def test_single_plan_generation_is_one_graph_launch(N, monkeypatch):
         np.testing.assert_array_equal(e2[k], g2[k], err_msg=k)
 
 
-def test_particle_placement_keeps_every_particles_result(monkeypatch):
+@pytest.mark.parametrize("n", [200, 400])  # fewer / more particles than the 296 resident CTAs
+def test_particle_placement_keeps_every_particles_result(n, monkeypatch):
     """Particle placement (on by default for the register kernel): the CTAs
     take particles in an order predicted from the plan's history (heaviest
     FIC work on the CTAs alone on an SM, the lightest on the second CTA of an
     SM).  Placement changes only where a particle runs, so every particle's
     results must equal those of the unplaced plan (BNM_B200_PLACE=0), bit for
-    bit, with more particles than SMs (paired and lone CTAs) and on the graph
-    path."""
-    N, n = 20, 200
+    bit, with more particles than SMs (paired and lone CTAs), with more
+    particles than resident CTAs (CTAs claim again from both ends until the
+    claims meet) and on the graph path."""
+    N = 20
     sc = synth.make_sc(N, 0.3, 6)
     cfg = B.Config(nodes=N, max_sims=n, time_steps=12000, bold_tr=500, window_size=10, window_step=2,
                    bold_remove_s=2)
