@@ -115,6 +115,9 @@ def lib():
         L.bnm_cmaes_best.argtypes = [vp, vp, vp]
         L.bnm_cmaes_set_samples.argtypes = [vp, vp]
         L.bnm_cmaes_state.argtypes = [vp, vp, vp, vp]
+        L.bnm_cmaes_save.argtypes = [vp, C.c_char_p]
+        L.bnm_cmaes_load.argtypes = [C.c_char_p, C.POINTER(vp)]
+        L.bnm_cmaes_params_of.argtypes = [vp, C.POINTER(_CmaesParams)]
         _lib = L
     return _lib
 
@@ -520,3 +523,23 @@ class CMAES:
         m, s, Cm = np.zeros(self.dim), C.c_double(), np.zeros((self.dim, self.dim))
         lib().bnm_cmaes_state(self._h, _ptr(m), C.byref(s), _ptr(Cm))
         return m, s.value, Cm
+
+    def save(self, path: str):
+        """Checkpoint the whole optimiser state to path (bnm_cmaes_save)."""
+        rc = lib().bnm_cmaes_save(self._h, os.fsencode(path))
+        if rc != 0:
+            raise BnmError(BNM_EINVAL, f"cannot write CMA-ES checkpoint {path} ({rc})")
+
+    @classmethod
+    def load(cls, path: str) -> "CMAES":
+        """An optimiser resumed from a checkpoint (bnm_cmaes_load)."""
+        h = C.c_void_p()
+        rc = lib().bnm_cmaes_load(os.fsencode(path), C.byref(h))
+        if rc != 0:
+            raise BnmError(BNM_EINVAL, f"cannot read CMA-ES checkpoint {path} ({rc})")
+        self = cls.__new__(cls)
+        self._h = h
+        p = _CmaesParams()
+        lib().bnm_cmaes_params_of(h, C.byref(p))
+        self.lam, self.dim, self.it_max = p.lambda_, p.dimension, p.it_max
+        return self

@@ -14,10 +14,14 @@
 // largest-magnitude component made positive.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <random>
+#include <string>
+#include <type_traits>
+#include <utility>
 #include <vector>
 #include "../../include/bnm_b200.h"
 
@@ -485,9 +489,129 @@ extern "C" int bnm_cmaes_best(const bnm_cmaes* c, double* x, double* value) {
     return 0;
 }
 
+extern "C" int bnm_cmaes_params_of(const bnm_cmaes* c, bnm_cmaes_params* out) {
+    if (!c || !out) return 1;
+    *out = c->P;
+    return 0;
+}
+
 extern "C" int bnm_cmaes_state(const bnm_cmaes* c, double* mean, double* sigma, double* C) {
     if (mean) std::copy(c->m.begin(), c->m.end(), mean);
     if (sigma) *sigma = c->sigma;
     if (C) std::copy(c->C.begin(), c->C.end(), C);
+    return 0;
+}
+
+// ------------------------------------------------------------ checkpoint
+// The optimiser's whole state in one file: a magic word and format version,
+// the parameters, the scalars and every vector with its length, doubles as
+// their exact bytes.  The random engines are seeded afresh inside each
+// sampling call (SeedMW and 11 + it), so they hold no state of their own.
+// No counterpart in the reference (its state is process-global).
+namespace {
+
+constexpr uint64_t kCkptMagic = 0x544b50434d424e42ull;  // "BNBMCPKT"
+constexpr uint32_t kCkptVersion = 1;
+
+struct Writer {
+    std::FILE* f;
+    bool ok = true;
+    void raw(const void* p, size_t n) { ok = ok && std::fwrite(p, 1, n, f) == n; }
+    template <typename T> void put(const T& v) { raw(&v, sizeof v); }
+    template <typename T> void vec(const std::vector<T>& v) {
+        put((uint64_t)v.size());
+        if (!v.empty()) raw(v.data(), v.size() * sizeof(T));
+    }
+};
+
+struct Reader {
+    std::FILE* f;
+    bool ok = true;
+    void raw(void* p, size_t n) { ok = ok && std::fread(p, 1, n, f) == n; }
+    template <typename T> void get(T& v) { raw(&v, sizeof v); }
+    template <typename T> void vec(std::vector<T>& v, size_t expect) {
+        uint64_t n = 0;
+        get(n);
+        ok = ok && n == expect;
+        if (!ok) return;
+        v.assign(n, T());
+        if (n) raw(v.data(), n * sizeof(T));
+    }
+};
+
+template <typename IO, typename S>
+void scalars(IO& io, S& c) {
+    auto f = [&](auto& x) {
+        if constexpr (std::is_same_v<IO, Writer>)
+            io.put(x);
+        else
+            io.get(x);
+    };
+    f(c.lambda), f(c.mue), f(c.D), f(c.H), f(c.sigma), f(c.cc), f(c.ccov), f(c.csigma), f(c.dsigma), f(c.chiN),
+        f(c.muecov), f(c.mueeff), f(c.c1), f(c.cmue), f(c.it), f(c.penalty), f(c.cancel), f(c.hsigma);
+}
+
+}  // namespace
+
+extern "C" int bnm_cmaes_save(const bnm_cmaes* c, const char* path) {
+    if (!c || !path) return 1;
+    const std::string tmp = std::string(path) + ".tmp";
+    std::FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return 2;
+    Writer w{f};
+    w.put(kCkptMagic);
+    w.put(kCkptVersion);
+    w.put(c->P);
+    scalars(w, *c);
+    for (const auto* v : {&c->weights, &c->Gamma, &c->lb, &c->ub, &c->ksi, &c->psigma, &c->pc, &c->m, &c->mpref,
+                          &c->malt, &c->IQAhist, &c->CBVfeas, &c->CBGVariables, &c->ww, &c->kk, &c->BDz, &c->Temp,
+                          &c->corr, &c->corrraw, &c->Helper, &c->tVektor, &c->C, &c->B, &c->Dm, &c->Vars, &c->Feas,
+                          &c->Pref})
+        w.vec(*v);
+    w.vec(c->indexx);
+    const bool ok = w.ok && std::fflush(f) == 0;
+    if (std::fclose(f) != 0 || !ok) {
+        std::remove(tmp.c_str());
+        return 2;
+    }
+    // the file appears whole or not at all
+    return std::rename(tmp.c_str(), path) == 0 ? 0 : 2;
+}
+
+extern "C" int bnm_cmaes_load(const char* path, bnm_cmaes** out) {
+    if (!path || !out) return 1;
+    std::FILE* f = std::fopen(path, "rb");
+    if (!f) return 2;
+    Reader r{f};
+    uint64_t magic = 0;
+    uint32_t version = 0;
+    r.get(magic);
+    r.get(version);
+    bnm_cmaes* c = new bnm_cmaes();
+    r.get(c->P);
+    r.ok = r.ok && magic == kCkptMagic && version == kCkptVersion;
+    if (r.ok) scalars(r, *c);
+    const size_t L = r.ok ? (size_t)std::max(c->lambda, 0) : 0, D = r.ok ? (size_t)std::max(c->D, 0) : 0;
+    r.ok = r.ok && L >= 2 && D >= 1 && c->lambda == c->P.lambda && c->D == c->P.dimension && c->H >= 1 &&
+           c->P.early_stop_gens >= 1;
+    const size_t H = r.ok ? (size_t)c->H : 0, E = r.ok ? (size_t)c->P.early_stop_gens : 0;
+    const std::pair<std::vector<double>*, size_t> vs[] = {
+        {&c->weights, L}, {&c->Gamma, D},  {&c->lb, D},       {&c->ub, D},           {&c->ksi, D},
+        {&c->psigma, D},  {&c->pc, D},     {&c->m, D},        {&c->mpref, D},        {&c->malt, D},
+        {&c->IQAhist, H}, {&c->CBVfeas, D + 1}, {&c->CBGVariables, D + 1}, {&c->ww, L}, {&c->kk, L},
+        {&c->BDz, D},     {&c->Temp, D},   {&c->corr, L},     {&c->corrraw, L},      {&c->Helper, D},
+        {&c->tVektor, E}, {&c->C, D * D},  {&c->B, D * D},    {&c->Dm, D * D},       {&c->Vars, D * L},
+        {&c->Feas, D * L}, {&c->Pref, D * L}};
+    for (const auto& v : vs)
+        if (r.ok) r.vec(*v.first, v.second);
+    if (r.ok) r.vec(c->indexx, L);
+    char extra;
+    r.ok = r.ok && std::fread(&extra, 1, 1, f) == 0;  // nothing after the state
+    std::fclose(f);
+    if (!r.ok) {
+        delete c;
+        return 3;
+    }
+    *out = c;
     return 0;
 }

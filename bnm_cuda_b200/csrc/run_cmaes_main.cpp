@@ -16,7 +16,17 @@
 // selects the integrator arithmetic and BNM_B200_GRAM=f32|bf16|bf16x3 the FC /
 // FCD Gram arithmetic (default bf16x3 with f32, f32 with the reference-order
 // modes).
+//
+// Checkpoint / resume (no counterpart in the reference): with
+// BNM_B200_CHECKPOINT=<file> the driver saves the CMA-ES state and the length
+// of its log after every generation; a later run with the same arguments and
+// file continues from there (the log is cut back to that length and
+// appended), and gives the log and result files of an uninterrupted run.
+// BNM_B200_MAX_GENERATIONS=<k> stops after k generations of this process
+// (exit status 75, the checkpoint saved), for time-limited jobs.
 #include <sys/stat.h>
+#include <sys/types.h>
+#include <unistd.h>
 
 #include <algorithm>
 #include <chrono>
@@ -91,6 +101,58 @@ void write_row(const std::string& path, const double* v, int n) {
     if (!f) return;
     for (int j = 0; j < n; j++) std::fprintf(f, "%f ", v[j]);
     std::fclose(f);
+}
+
+// Driver checkpoint: one line "bnm_b200 driver checkpoint 1 <log bytes>"
+// followed by the CMA-ES state as bnm_cmaes_save writes it; the file is
+// written under a temporary name and renamed into place.
+constexpr const char* kCkptTag = "bnm_b200 driver checkpoint 1";
+
+bool slurp(const std::string& path, std::string* out) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) return false;
+    std::ostringstream ss;
+    ss << f.rdbuf();
+    *out = ss.str();
+    return true;
+}
+
+bool write_checkpoint(const std::string& path, const bnm_cmaes* es, long log_bytes) {
+    const std::string state = path + ".cmaes", tmp = path + ".tmp";
+    std::string bytes;
+    if (bnm_cmaes_save(es, state.c_str()) != 0 || !slurp(state, &bytes)) return false;
+    std::remove(state.c_str());
+    FILE* f = std::fopen(tmp.c_str(), "wb");
+    if (!f) return false;
+    bool ok = std::fprintf(f, "%s %ld\n", kCkptTag, log_bytes) > 0 &&
+              std::fwrite(bytes.data(), 1, bytes.size(), f) == bytes.size() && std::fflush(f) == 0;
+    ok = std::fclose(f) == 0 && ok;
+    return ok && std::rename(tmp.c_str(), path.c_str()) == 0;
+}
+
+// 0: no checkpoint (a fresh run) or a checkpoint read into *es and *log_bytes;
+// 1: a file that is not a driver checkpoint (reported).
+int read_checkpoint(const std::string& path, bnm_cmaes** es, long* log_bytes) {
+    std::string all;
+    if (!slurp(path, &all)) return 0;
+    const size_t nl = all.find('\n');
+    const std::string tag = kCkptTag;
+    char* end = nullptr;
+    const long n = nl == std::string::npos || all.compare(0, tag.size(), tag) != 0
+                       ? -1
+                       : std::strtol(all.c_str() + tag.size(), &end, 10);
+    const std::string state = path + ".cmaes";
+    if (n >= 0 && end == all.c_str() + nl) {
+        std::ofstream(state, std::ios::binary).write(all.data() + nl + 1, (std::streamsize)(all.size() - nl - 1));
+        const int rc = bnm_cmaes_load(state.c_str(), es);
+        std::remove(state.c_str());
+        if (rc == 0) {
+            *log_bytes = n;
+            return 0;
+        }
+    }
+    std::fprintf(stderr, "Error: %s is not a checkpoint of this driver\n", path.c_str());
+    return 1;
 }
 
 }  // namespace
@@ -242,7 +304,16 @@ int main(int argc, char* argv[]) {
     prefix += "_het-" + d.het_params_str + "_SeedMW-" + std::to_string(d.SeedMW) + "_SeedSim-" +
               std::to_string(d.rand_seed) + "_n-" + std::to_string(d.itMax) + "x" + std::to_string(d.lambda);
     const std::string log_path = cmaes_dir + "/" + prefix + ".txt", sims_prefix = sims_dir + "/" + prefix + "_";
-    FILE* log = std::fopen(log_path.c_str(), "w");
+    const char* ckpt_env = std::getenv("BNM_B200_CHECKPOINT");
+    const std::string ckpt = ckpt_env ? ckpt_env : "";
+    long resume_log_bytes = -1;
+    bnm_cmaes* resumed = nullptr;
+    if (!ckpt.empty() && read_checkpoint(ckpt, &resumed, &resume_log_bytes)) return 1;
+    if (resumed && truncate(log_path.c_str(), (off_t)resume_log_bytes) != 0) {
+        std::fprintf(stderr, "Error: cannot cut the log %s back to its checkpointed length\n", log_path.c_str());
+        return 1;
+    }
+    FILE* log = std::fopen(log_path.c_str(), resumed ? "a" : "w");
     if (!log) {
         std::fprintf(stderr, "Error opening log file %s\n", log_path.c_str());
         return 1;
@@ -251,11 +322,15 @@ int main(int argc, char* argv[]) {
         std::fprintf(log, fmt, a...);
         std::printf(fmt, a...);
     };
-    both("Running %dD CMAES\nSC: %s\nFC: %s\n", Dimension, d.sc_path.c_str(), d.fc_tril_path.c_str());
-    if (d.heterogeneous) both("Maps: %s\n", d.maps_path.c_str());
-    both("Free parameters: ");
-    for (auto& kv : d.param_mins) both("%s (%f-%f) ", kv.first.c_str(), kv.second, d.param_maxs[kv.first]);
-    both("\nFCD step %d, FCD window %d, Simulation random seed %d, CMAES random seed %d, sigma %f, alphacov %f, "
+    auto header = [&](const char* fmt, auto... a) {  // already in a resumed log
+        if (!resumed) std::fprintf(log, fmt, a...);
+        std::printf(fmt, a...);
+    };
+    header("Running %dD CMAES\nSC: %s\nFC: %s\n", Dimension, d.sc_path.c_str(), d.fc_tril_path.c_str());
+    if (d.heterogeneous) header("Maps: %s\n", d.maps_path.c_str());
+    header("Free parameters: ");
+    for (auto& kv : d.param_mins) header("%s (%f-%f) ", kv.first.c_str(), kv.second, d.param_maxs[kv.first]);
+    header("\nFCD step %d, FCD window %d, Simulation random seed %d, CMAES random seed %d, sigma %f, alphacov %f, "
          "gamma_scale %f, bound_soft_edge %f, Variante %d, early stop gens %d, early stop tol %f\n",
          d.window_step, d.window_size, d.rand_seed, d.SeedMW, cp.sigma, cp.alphacov, cp.gamma_scale,
          cp.bound_soft_edge, cp.variante, cp.early_stop_gens, cp.early_stop_tol);
@@ -311,10 +386,23 @@ int main(int argc, char* argv[]) {
     cp.seed_mw = d.SeedMW;
     cp.it_max = d.itMax;
     bnm_cmaes* es = nullptr;
-    if (bnm_cmaes_create(&cp, &es)) {
+    if (resumed) {
+        bnm_cmaes_params rp;
+        bnm_cmaes_params_of(resumed, &rp);
+        if (rp.lambda != cp.lambda || rp.dimension != cp.dimension || rp.seed_mw != cp.seed_mw ||
+            rp.it_max != cp.it_max || rp.variante != cp.variante || rp.sigma != cp.sigma) {
+            std::fprintf(stderr, "Error: checkpoint %s was written for other CMA-ES settings\n", ckpt.c_str());
+            return 1;
+        }
+        es = resumed;
+        std::printf("Resuming from %s at iteration %d\n", ckpt.c_str(), bnm_cmaes_iteration(es));
+    } else if (bnm_cmaes_create(&cp, &es)) {
         std::fprintf(stderr, "Error: bad CMA-ES settings\n");
         return 1;
     }
+    const char* mg = std::getenv("BNM_B200_MAX_GENERATIONS");
+    const int max_gens = mg ? std::atoi(mg) : 0;  // generations of this process (0: no limit)
+    int gens_here = 0;
     const int L = d.lambda, N = d.nodes;
     std::vector<double> G(L), wEE((size_t)L * N), wEI((size_t)L * N), wIE((size_t)L * N, 0.0);
     std::vector<double> feas((size_t)Dimension * L), cost(L), pen(L), total(L), penalized(L);
@@ -354,6 +442,21 @@ int main(int argc, char* argv[]) {
                 both("gof=%f,penalized_cost=%f\n", -total[i], penalized[i]);
         }
         it = new_it;
+        if (!ckpt.empty()) {
+            std::fflush(log);
+            if (!write_checkpoint(ckpt, es, std::ftell(log))) {
+                std::fprintf(stderr, "Error: cannot write checkpoint %s\n", ckpt.c_str());
+                return 1;
+            }
+        }
+        if (max_gens > 0 && ++gens_here >= max_gens && it < d.itMax) {
+            std::printf("Stopped after %d generations at iteration %d%s\n", gens_here, it,
+                        ckpt.empty() ? "" : "; rerun with the same checkpoint to continue");
+            std::fclose(log);
+            bnm_cmaes_destroy(es);
+            bnm_plan_destroy(plan);
+            return 75;  // EX_TEMPFAIL: incomplete, to be continued
+        }
     }
 
     // best feasible point, rerun and saved (run_CMAES.cpp:821-906, bnm.cu:771-833)

@@ -365,6 +365,18 @@ int bnm_cmaes_set_samples(bnm_cmaes *c, const double *raw);
 /* Best feasible point [dim] and its value (-cost, the reference's CBVfeas[D]). */
 int bnm_cmaes_best(const bnm_cmaes *c, double *x, double *value);
 int bnm_cmaes_state(const bnm_cmaes *c, double *mean, double *sigma, double *C);
+/* Checkpoint / resume (no counterpart in the reference, whose CMA-ES state is
+ * process-global, cmaes.cpp:69-126): bnm_cmaes_save writes the optimiser's
+ * whole state (parameters, counters, mean, paths, covariance and its
+ * decomposition, current samples, best-so-far and early-stop history; exact
+ * doubles) to path, through a temporary file renamed into place, so the file
+ * is whole or absent.  bnm_cmaes_load creates an optimiser from such a file;
+ * it samples and updates exactly as the one that was saved.  Returns 0, 1
+ * (null argument), 2 (file error) or 3 (not a checkpoint of this format). */
+int bnm_cmaes_save(const bnm_cmaes *c, const char *path);
+int bnm_cmaes_load(const char *path, bnm_cmaes **out);
+/* The parameters an optimiser was created (or saved) with. */
+int bnm_cmaes_params_of(const bnm_cmaes *c, bnm_cmaes_params *out);
 
 /* ------------------------------------------------------ MLP surrogate
  * No counterpart in the reference.  A ReLU MLP (in -> hidden x layers -> out)

@@ -58,3 +58,44 @@ def test_cli_runs_cmaes_and_writes_reference_files(tmp_path, golden, het):
         assert np.loadtxt(sims / (prefix + f + ".txt")).shape == (N,)
     assert (sims / (prefix + "fic_ntrials.txt")).read_text().endswith("of max 10")
     assert (sims / (prefix + "fic_failed.txt")).read_text() in ("0", "1")
+
+
+@pytest.mark.gpu
+def test_cli_checkpoint_resume_gives_the_uninterrupted_run(tmp_path, golden):
+    """BNM_B200_CHECKPOINT: a run stopped after two generations
+    (BNM_B200_MAX_GENERATIONS=2, exit status 75) and started again with the
+    same checkpoint writes the same log and best-simulation files as a run
+    that was never interrupted."""
+    g = golden["n10_t12s"]
+    N, T, TR, ws, step, remove, exc, nvr, seed = [int(v) for v in g["meta"]]
+    lam, it_max = 6, 5
+
+    def setup(name):
+        d = tmp_path / name / "sub-01"
+        d.mkdir(parents=True)
+        np.savetxt(d / "SC.txt", g["sc"])
+        np.savetxt(d / "sub-01_desc-FCtril.txt", g["emp_fc"])
+        np.savetxt(d / "sub-01_desc-FCDtril.txt", g["emp_fcd"])
+        args = [CLI, str(d / "SC.txt"), "same", str(d / "sub-01_desc-FCtril.txt"),
+                str(d / "sub-01_desc-FCDtril.txt"), "none", str(N), "0.5-3.5", "0.05-0.5", "0.05-0.5", "0", "none",
+                str(T), str(TR), str(step), str(ws), "410", str(lam), str(it_max), "1"]
+        return d, args
+
+    env = dict(os.environ, BNM_BOLD_REMOVE=str(remove))
+    da, args = setup("straight")
+    r = subprocess.run(args, capture_output=True, text=True, env=env, timeout=600)
+    assert r.returncode == 0, r.stderr + r.stdout
+    db, args = setup("resumed")
+    ck = str(tmp_path / "resumed" / "run.ckpt")
+    r = subprocess.run(args, capture_output=True, text=True, env=dict(env, BNM_B200_CHECKPOINT=ck,
+                                                                      BNM_B200_MAX_GENERATIONS="2"), timeout=600)
+    assert r.returncode == 75, r.stderr + r.stdout
+    assert os.path.exists(ck) and "Stopped after 2 generations" in r.stdout
+    r = subprocess.run(args, capture_output=True, text=True, env=dict(env, BNM_B200_CHECKPOINT=ck), timeout=600)
+    assert r.returncode == 0, r.stderr + r.stdout
+    assert "Resuming from" in r.stdout
+    for sub in ("cmaes_gpu", "sims_gpu"):
+        fa, fb = sorted((da / "SC" / sub).iterdir()), sorted((db / "SC" / sub).iterdir())
+        assert [f.name for f in fa] == [f.name for f in fb] and fa
+        for x, y in zip(fa, fb):
+            assert x.read_text().replace(str(da), str(db)) == y.read_text(), x.name

@@ -122,3 +122,48 @@ def test_cmaes_reproduces_reference_bit_for_bit(name, golden):
     np.testing.assert_array_equal(x, g["best"][:dim])
     assert v == g["best"][dim]
     assert c.iteration >= it_max
+
+
+@pytest.mark.parametrize("variante", [6, 16])
+def test_cmaes_checkpoint_resumes_bit_for_bit(variante, tmp_path):
+    """bnm_cmaes_save after generation 5, bnm_cmaes_load into a new optimiser:
+    the resumed run samples, penalises and keeps its best exactly as the
+    uninterrupted one through generation 11."""
+    def cost(x):  # [dim][lambda] -> [lambda]
+        return ((x - 0.3) ** 2).sum(0) + 0.01 * np.sin(13 * x).sum(0)
+
+    path = str(tmp_path / "cmaes.ckpt")
+    a = B.CMAES(16, 3, 5, 40, from_env=False, variante=variante)
+    hist = []
+    for g in range(12):
+        f, r, p = a.samples()
+        it, pen = a.tell(cost(f))
+        hist.append((f, r, p, it, pen, *a.best(), *a.state()))
+        if g == 5:
+            a.save(path)
+            assert not os.path.exists(path + ".tmp")
+    b = B.CMAES.load(path)
+    assert (b.lam, b.dim, b.it_max) == (16, 3, 40)
+    assert b.iteration == hist[5][3]
+    for g in range(6, 12):
+        f, r, p = b.samples()
+        it, pen = b.tell(cost(f))
+        got = (f, r, p, it, pen, *b.best(), *b.state())
+        for x, y in zip(got, hist[g]):
+            np.testing.assert_array_equal(x, y)
+
+
+def test_cmaes_checkpoint_rejects_other_files(tmp_path):
+    a = B.CMAES(8, 2, 1, 10, from_env=False)
+    good = str(tmp_path / "good.ckpt")
+    a.save(good)
+    data = open(good, "rb").read()
+    for name, content in (("short", data[:-8]), ("long", data + b"\0"), ("magic", b"X" + data[1:])):
+        bad = str(tmp_path / name)
+        open(bad, "wb").write(content)
+        with pytest.raises(B.BnmError):
+            B.CMAES.load(bad)
+    with pytest.raises(B.BnmError):
+        B.CMAES.load(str(tmp_path / "missing.ckpt"))
+    with pytest.raises(B.BnmError):
+        a.save(str(tmp_path / "no" / "such" / "dir.ckpt"))
