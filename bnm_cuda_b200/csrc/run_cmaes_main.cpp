@@ -24,6 +24,9 @@
 // appended), and gives the log and result files of an uninterrupted run.
 // BNM_B200_MAX_GENERATIONS=<k> stops after k generations of this process
 // (exit status 75, the checkpoint saved), for time-limited jobs.
+// BNM_B200_METRICS=<file> appends one JSON line per generation (wall time,
+// simulations per second, the device's stage times, the generation's best
+// cost and the best fit so far).
 #include <sys/stat.h>
 #include <sys/types.h>
 #include <unistd.h>
@@ -400,6 +403,12 @@ int main(int argc, char* argv[]) {
         std::fprintf(stderr, "Error: bad CMA-ES settings\n");
         return 1;
     }
+    const char* me = std::getenv("BNM_B200_METRICS");  // JSON-lines sidecar, appended
+    FILE* metrics = me ? std::fopen(me, "a") : nullptr;
+    if (me && !metrics) {
+        std::fprintf(stderr, "Error opening metrics file %s\n", me);
+        return 1;
+    }
     const char* mg = std::getenv("BNM_B200_MAX_GENERATIONS");
     const int max_gens = mg ? std::atoi(mg) : 0;  // generations of this process (0: no limit)
     int gens_here = 0;
@@ -428,10 +437,29 @@ int main(int argc, char* argv[]) {
         auto t1 = std::chrono::high_resolution_clock::now();
         if (bnm_run(plan, L, G.data(), wEE.data(), wEI.data(), d.do_fic ? nullptr : wIE.data(), &out))
             die("run_simulations");
-        std::printf("took %lf s\n",
-                    std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t1).count());
+        const double gen_s = std::chrono::duration<double>(std::chrono::high_resolution_clock::now() - t1).count();
+        std::printf("took %lf s\n", gen_s);
         for (int i = 0; i < L; i++) total[i] = cost[i] + (d.do_fic ? pen[i] : 0.0);
+        const int this_it = it;
         const int new_it = bnm_cmaes_tell(es, total.data(), penalized.data());
+        if (metrics) {  // one JSON line per generation
+            double ms[6];
+            bnm_last_timings(plan, ms);
+            double bx = 0;
+            bnm_cmaes_best(es, nullptr, &bx);
+            std::fprintf(metrics,
+                         "{\"iteration\": %d, \"simulations\": %d, \"wall_s\": %.6f, \"sims_per_s\": %.4f, "
+                         "\"device_ms\": {\"fic\": %.4f, \"integrate\": %.4f, \"fc_window\": %.4f, "
+                         "\"fcd_ks\": %.4f, \"gof\": %.4f, \"total\": %.4f}, \"generation_best_cost\": %.9g, "
+                         "\"best_gof\": %.9g, \"graph_launch\": %s}\n",
+                         this_it, L, gen_s, L / gen_s, ms[0], ms[1], ms[2], ms[3], ms[4], ms[5],
+                         *std::min_element(total.begin(), total.end()), bx, [&] {
+                             int32_t g = 0;
+                             bnm_plan_graph(plan, &g);
+                             return g ? "true" : "false";
+                         }());
+            std::fflush(metrics);
+        }
         for (int i = 0; i < L; i++) {
             both("\t IndPar %d: ", i);
             auto c = params_of(feas.data(), L, i);
@@ -453,6 +481,7 @@ int main(int argc, char* argv[]) {
             std::printf("Stopped after %d generations at iteration %d%s\n", gens_here, it,
                         ckpt.empty() ? "" : "; rerun with the same checkpoint to continue");
             std::fclose(log);
+            if (metrics) std::fclose(metrics);
             bnm_cmaes_destroy(es);
             bnm_plan_destroy(plan);
             return 75;  // EX_TEMPFAIL: incomplete, to be continued
@@ -510,6 +539,7 @@ int main(int argc, char* argv[]) {
         both("gof=%f,fic_penalty=%f,gof_fic_penalty=%f\n", -cost[0], pen[0], best_val);
     else
         both("gof=%f\n", best_val);
+    if (metrics) std::fclose(metrics);
     std::fclose(log);
     bnm_cmaes_destroy(es);
     bnm_plan_destroy(plan);

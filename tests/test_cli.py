@@ -1,6 +1,7 @@
 """The drop-in CLI (bnm_cuda_b200/run_CMAES_gpu) on a small synthetic case:
 same arguments as the reference's run_CMAES (run_CMAES.cpp:192-218), same
 output directories, log lines and best-simulation files (bnm.cu:771-833)."""
+import json
 import os
 import re
 import subprocess
@@ -83,8 +84,15 @@ def test_cli_checkpoint_resume_gives_the_uninterrupted_run(tmp_path, golden):
 
     env = dict(os.environ, BNM_BOLD_REMOVE=str(remove))
     da, args = setup("straight")
-    r = subprocess.run(args, capture_output=True, text=True, env=env, timeout=600)
+    metrics = tmp_path / "metrics.jsonl"
+    r = subprocess.run(args, capture_output=True, text=True, env=dict(env, BNM_B200_METRICS=str(metrics)),
+                       timeout=600)
     assert r.returncode == 0, r.stderr + r.stdout
+    lines = [json.loads(x) for x in metrics.read_text().splitlines()]  # BNM_B200_METRICS: one line per generation
+    assert [m["iteration"] for m in lines] == list(range(1, it_max))
+    for m in lines:
+        assert m["simulations"] == lam and m["sims_per_s"] > 0 and m["device_ms"]["total"] > 0
+        assert np.isfinite(m["best_gof"]) and np.isfinite(m["generation_best_cost"])
     db, args = setup("resumed")
     ck = str(tmp_path / "resumed" / "run.ckpt")
     r = subprocess.run(args, capture_output=True, text=True, env=dict(env, BNM_B200_CHECKPOINT=ck,
