@@ -167,3 +167,33 @@ def test_cmaes_checkpoint_rejects_other_files(tmp_path):
         B.CMAES.load(str(tmp_path / "missing.ckpt"))
     with pytest.raises(B.BnmError):
         a.save(str(tmp_path / "no" / "such" / "dir.ckpt"))
+
+
+def test_cmaes_cancels_on_a_covariance_that_is_not_positive(tmp_path):
+    """Host-side fault injection through the checkpoint format: a saved state
+    whose covariance has a negative diagonal entry makes the next
+    bnm_cmaes_tell stop the run (iteration = it_max, as the reference's
+    CMAES_Points cancels, cmaes.cpp:402-420) instead of sampling from it."""
+    import ctypes
+
+    a = B.CMAES(8, 2, 3, 30, from_env=False)
+    for _ in range(3):
+        f, _, _ = a.samples()
+        a.tell(((f - 0.4) ** 2).sum(0))
+    path = tmp_path / "ok.ckpt"
+    a.save(str(path))
+    data = bytearray(path.read_bytes())
+    # magic (8 bytes), version (4), the parameter struct, 4 ints, 10 doubles,
+    # 4 ints, then length-prefixed vectors; the covariance C is the 22nd
+    off = 8 + 4 + ctypes.sizeof(B._CmaesParams) + 16 + 80 + 16
+    for _ in range(21):
+        n = int.from_bytes(data[off:off + 8], "little")
+        off += 8 + 8 * n
+    assert int.from_bytes(data[off:off + 8], "little") == 4  # D x D
+    data[off + 8:off + 16] = np.float64(-1.0).tobytes()  # C[0][0]
+    bad = tmp_path / "bad.ckpt"
+    bad.write_bytes(bytes(data))
+    b = B.CMAES.load(str(bad))
+    f, _, _ = b.samples()
+    it, _ = b.tell(((f - 0.4) ** 2).sum(0))
+    assert it == 30
