@@ -473,7 +473,7 @@ def run_surrogate(args):
             mlp.set_params(trained)
             screen = S.run_cmaes(plan, bounds, 64, args.generations, seed=seed, mlp=mlp, spec=spec, oversample=8,
                                  holdout_spearman=info["holdout_spearman"])
-            # the north star's target: within 0.01 of plain CMA-ES's final best
+            # the target: within 0.01 of plain CMA-ES's final best
             target = plain["best"] + 0.01
             tp_, ts_ = to_target(plain, target), to_target(screen, target)
             # and the better of the two final bests + 0.01: a run that never gets there loses outright
