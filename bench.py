@@ -669,6 +669,10 @@ def run_subjects(args):
                 es.tell(cost)
         shapes = [p.integrator() for p in plans]
         launches = sum(p.gram_timing()["launches"] for p in plans)
+        # the last generation's stage times per subject (events on each subject's stream, inside the graph:
+        # a stage's time includes waiting for SMs that other subjects hold)
+        subject_ms = [{k: round(float(v), 1) for k, v in p.timings().items()} for p in plans]
+        max_trials = [int(r["fic_ntrials"].max()) for r in res]
     timed_ms, timed_wall = float(np.sum(gen_ms[1:])), float(np.sum(walls[1:]))
     n_timed = len(gen_ms) - 1
     print(json.dumps({
@@ -684,7 +688,8 @@ def run_subjects(args):
                 "d2h_bytes_per_step": sum(8 * lam * (5 + N) + 12 * lam for N in nodes)},
         "gpu_launches": launches * n_timed,
         "generation_ms": gen_ms, "graph_launched": graph, "first_generation_eager_ms": gen_ms[0],
-        "mean_fic_trials": trials[-1], "best_cost": best, "clocks": clk.summary(),
+        "mean_fic_trials": trials[-1], "max_fic_trials": max_trials, "subject_stage_ms": subject_ms,
+        "best_cost": best, "clocks": clk.summary(),
     }))
     for p in plans:
         p.close()
