@@ -555,10 +555,10 @@ def run_precision(args):
     import bnm_cuda_b200 as B
     from bnm_cuda_b200 import synth
 
-    # --particles / --model-ms (profiling knobs) replace the 64 particles and 600 s when given
+    # --particles / --model-ms / --nodes (profiling knobs) replace the 64 particles, 600 s and 400 nodes
     n = args.particles if args.particles != DEFAULT_SIMS else 64
     T = args.model_ms if args.model_ms != DEFAULT_T_MS else 600_000
-    N, TRp, WSp, STEPp = 400, 500, 44, 1
+    N, TRp, WSp, STEPp = args.nodes, 500, 44, 1
     sc = synth.make_sc(N, 0.1, 0)
     G, wEE, wEI = synth.uniform_params(n, N, 1)
     cfg = B.Config(nodes=N, max_sims=n, time_steps=T, bold_tr=TRp, window_size=WSp, window_step=STEPp,
@@ -610,7 +610,7 @@ def run_precision(args):
     print(json.dumps({
         "metric": "sims/s", "value": n / (tm["total"] / 1e3), "unit": "sims/s", "n_gpus": 1, "steps": 1,
         "higher_is_better": True, "data": "synthetic", "dtype": "f32 integration; FC/FCD Grams f32 / bf16 / bf16x3",
-        "config": {"workload": f"precision-stress-N400-{T // 1000}s-x{n}", "nodes": N, "particles": n, "model_time_ms": T,
+        "config": {"workload": f"precision-stress-N{N}-{T // 1000}s-x{n}", "nodes": N, "particles": n, "model_time_ms": T,
                    "tr_ms": TRp, "window": WSp, "step": STEPp, "windows": W, "pairs": P, "fcd_entries": s["n_fcd"],
                    "sc_density": 0.1, "integrator": integ, "checked_particles": k},
         "wall_s": wall, "stage_ms": tm, "precision": table,
@@ -709,6 +709,7 @@ def main():
                          "N = 68..400 in one graph per generation")
     ap.add_argument("--subject-generations", type=int, default=4, help="subjects: generations (first is eager)")
     ap.add_argument("--check-sims", type=int, default=4, help="precision: particles checked against FP64")
+    ap.add_argument("--nodes", type=int, default=400, help="precision: profiling knob, node count (default 400)")
     ap.add_argument("--gram", default="bf16x3", choices=["f32", "bf16", "bf16x3"],
                     help="generation: FC/FCD Gram arithmetic")
     ap.add_argument("--train-sims", type=int, default=20_000)
